@@ -1,0 +1,491 @@
+// Panel factorisation for stage 1: tall-skinny QR (m x 32) and the compact
+// Householder form Q = I - W Y^T.
+//
+// Reference: panelQR<double> (api/panelQR.cu:54-108) = hou_tsqr_panel<128,32>
+// (api/inc/TallShinnyQR.h:9-133, leaf kernel util/inc/kernelQR.h:215-414),
+// then IminusQ, cusolverDnDgetrf without pivoting, getLower and a Dtrsm.
+//
+// Same numerics, B200 structure:
+//  * The TSQR tree has the reference's shape (128-row tiles, R factors
+//    stacked 32 rows per child, fan-in 4), but runs as ONE up-sweep kernel:
+//    each CTA factors its tile in registers/shared memory, publishes its R,
+//    and the last child to arrive at a parent (atomic counter) goes on to
+//    factor the parent.  Nobody waits, so there is no grid barrier and no
+//    spin.  The reference launches one kernel plus batched GEMMs per level.
+//  * One finishing kernel forms each tile's rows of the explicit thin Q
+//    (leaf Q times the 32x32 path product down the tree, right to left as
+//    the reference's recursion), and in the same pass rebuilds the Householder
+//    form: the unpivoted LU of (I - Q)[0:32] (recomputed redundantly by each
+//    CTA from tile 0's data, so no inter-CTA dependency), Y = (I-Q) U^{-1}
+//    (rows >= 32) or L1 (rows < 32), W = (I-Q) L1^{-T}.  This replaces the
+//    getrf + getLower + trsm + copy kernels.
+//  * In the sy2sb pipeline the finishing kernel writes Y and W straight into
+//    dY/dW and the band (R over zeros) into dA (the reference's copyMatrix +
+//    getU, api/zy_zy_sy2sb.cu:122-125).
+#include "common.cuh"
+#include "panel_qr.cuh"
+
+namespace evd {
+
+namespace {
+
+constexpr int kTile = 128;   // rows per TSQR tile (reference: M = 128)
+constexpr int kNB = 32;      // panel width (reference: N = 32)
+constexpr int kThreads = 256;
+constexpr int kMaxLevels = 16;
+
+struct TsqrPlan {
+  int m;
+  int nlev;                 // number of levels; level nlev-1 is the root (1 tile)
+  int T[kMaxLevels];        // tiles at each level
+  int rows[kMaxLevels];     // rows of the matrix factored at each level
+  long soff[kMaxLevels];    // offset (doubles) of stack S_L in ws (L >= 1)
+  int coff[kMaxLevels];     // offset of the arrival counters of level L (L >= 1)
+  long qtop_off;            // 32x32 copy of tile 0's leaf Q rows 0..31
+  long cnt_off;             // int counters start (in doubles, aligned)
+  int ncnt;
+  long total;               // doubles
+};
+
+TsqrPlan make_plan(long m) {
+  TsqrPlan p{};
+  p.m = (int)m;
+  int L = 0;
+  p.rows[0] = (int)m;
+  p.T[0] = ceil_div_i(m, kTile);
+  long off = 0;
+  int coff = 0;
+  while (p.T[L] > 1 && L + 1 < kMaxLevels) {
+    p.rows[L + 1] = kNB * p.T[L];
+    p.T[L + 1] = ceil_div_i(p.rows[L + 1], kTile);
+    p.soff[L + 1] = off;
+    off += (long)p.rows[L + 1] * kNB;
+    p.coff[L + 1] = coff;
+    coff += p.T[L + 1];
+    ++L;
+  }
+  p.nlev = L + 1;
+  p.qtop_off = off;
+  off += kNB * kNB;
+  p.cnt_off = off;
+  p.ncnt = coff;
+  off += (coff + 1) / 2 + 2;  // ints packed two per double
+  p.total = off;
+  return p;
+}
+
+// Householder QR of one tile (mm <= 128 rows, 32 columns) held in registers:
+// warp w owns columns 4w..4w+3, lane l owns rows l, l+32, l+64, l+96.
+// Writes R (32x32, upper; diag = -sign(x0)||x||) to Rdst and the explicit thin
+// Q over the tile rows back to src.  Same steps as my_hou_kernel<128,32>.
+struct TileSmem {
+  double V[kNB * kTile];  // Householder vectors, column j at V[j*128 ..]
+  double us[kTile];
+  double RR[kNB];
+};
+
+__device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, TileSmem& sm,
+                        double* qtop_copy) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double a[4][4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int row = lane + 32 * i;
+      a[c][i] = (row < mm) ? __ldcg(src + row + (long)(4 * warp + c) * ld) : 0.0;
+    }
+
+  for (int j = 0; j < kNB; ++j) {
+    const int ow = j >> 2, oc = j & 3;
+    if (warp == ow) {
+      double x[4], ss = 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        int row = lane + 32 * i;
+        double v = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c == oc) v = a[c][i];
+        x[i] = (row >= j && row < mm) ? v : 0.0;
+        ss = fma(x[i], x[i], ss);
+      }
+      double nrm2 = warp_sum(ss);
+      double nrm = sqrt(nrm2);
+      double scale = (nrm2 > 0.0) ? 1.0 / nrm : 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) sm.us[lane + 32 * i] = x[i] * scale;
+      __syncwarp();
+      double u0 = sm.us[j];
+      double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
+      double s2 = (nrm2 > 0.0) ? 1.0 / sqrt(fabs(u0n)) : 0.0;
+      if (lane == 0) sm.RR[j] = (u0 >= 0.0) ? -nrm : nrm;
+      __syncwarp();
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        int row = lane + 32 * i;
+        double u = sm.us[row];
+        if (row == j) u = u0n;
+        u *= s2;
+        if (nrm2 == 0.0) u = 0.0;
+        sm.us[row] = u;
+        sm.V[j * kTile + row] = u;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c == oc && row >= j) a[c][i] = u;
+      }
+    }
+    __syncthreads();
+    double uv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) uv[i] = sm.us[lane + 32 * i];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (4 * warp + c > j) {
+        double p = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) p = fma(uv[i], a[c][i], p);
+        double dot = warp_sum(p);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
+      }
+    }
+    __syncthreads();
+  }
+
+  // R: row k = lane (i = 0), column h = 4w + c
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    int h = 4 * warp + c;
+    double r = (lane < h) ? a[c][0] : ((lane == h) ? sm.RR[h] : 0.0);
+    Rdst[lane + (long)h * ldR] = r;
+  }
+
+  // explicit thin Q = H_0 ... H_31 I[:, :32], accumulated backwards
+  double q[4][4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[c][i] = (lane + 32 * i == 4 * warp + c) ? 1.0 : 0.0;
+  for (int j = kNB - 1; j >= 0; --j) {
+    double uv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      if (4 * warp + c >= j) {
+        double p = 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) p = fma(uv[i], q[c][i], p);
+        double dot = warp_sum(p);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) q[c][i] = fma(-dot, uv[i], q[c][i]);
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int row = lane + 32 * i;
+      if (row < mm) {
+        src[row + (long)(4 * warp + c) * ld] = q[c][i];
+        if (qtop_copy && row < kNB) qtop_copy[row + (4 * warp + c) * kNB] = q[c][i];
+      }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) tsqr_up_kernel(const TsqrPlan plan, double* A,
+                                                           long lda, double* ws, double* Rout,
+                                                           long ldr) {
+  __shared__ TileSmem sm;
+  __shared__ int is_last;
+  int* cnt = reinterpret_cast<int*>(ws + plan.cnt_off);
+  int level = 0, idx = blockIdx.x;
+  for (;;) {
+    double* src;
+    long ld;
+    if (level == 0) {
+      src = A + (long)idx * kTile;
+      ld = lda;
+    } else {
+      src = ws + plan.soff[level] + (long)idx * kTile;
+      ld = plan.rows[level];
+    }
+    int mm = min(kTile, plan.rows[level] - idx * kTile);
+    const bool root = (plan.T[level] == 1);
+    double* Rdst;
+    long ldR;
+    if (root) {
+      Rdst = Rout;
+      ldR = ldr;
+    } else {
+      Rdst = ws + plan.soff[level + 1] + (long)idx * kNB;
+      ldR = plan.rows[level + 1];
+    }
+    double* qtop = (level == 0 && idx == 0) ? ws + plan.qtop_off : nullptr;
+    tile_qr(src, ld, mm, Rdst, ldR, sm, qtop);
+    if (root) break;
+    const int parent = idx / 4;
+    const int nch = min(4, plan.T[level] - 4 * parent);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int* c = cnt + plan.coff[level + 1] + parent;
+      int old = atomicAdd(c, 1);
+      is_last = (old == nch - 1);
+      if (is_last) *c = 0;  // self-reset for the next panel
+    }
+    __syncthreads();
+    if (!is_last) break;
+    __threadfence();
+    ++level;
+    idx = parent;
+  }
+}
+
+struct FinishSmem {
+  double M[kNB * (kNB + 1)];
+  double T[kNB * (kNB + 1)];
+  double B[kNB * (kNB + 1)];
+  double LU[kNB * (kNB + 1)];
+};
+
+// C = Bm * M (32x32x32) into Out (all padded stride 33), 256 threads.
+__device__ void mul32(const double* Bm, const double* M, double* Out) {
+  for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+    int r = e & 31, c = e >> 5;
+    double s = 0.0;
+#pragma unroll 8
+    for (int k = 0; k < kNB; ++k) s = fma(Bm[r * 33 + k], M[k * 33 + c], s);
+    Out[r * 33 + c] = s;
+  }
+}
+
+// Path product for leaf tile t: M = B_1 (B_2 (... B_top)) with
+// B_L = S_L[32*idx_{L-1} : +32, :].  Result in sm.M.
+__device__ void path_product(const TsqrPlan& plan, const double* ws, int t, FinishSmem& sm) {
+  int idxs[kMaxLevels];
+  idxs[0] = t;
+  for (int L = 1; L < plan.nlev; ++L) idxs[L] = idxs[L - 1] / 4;
+  for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+    int r = e & 31, c = e >> 5;
+    sm.M[r * 33 + c] = (r == c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int L = plan.nlev - 1; L >= 1; --L) {
+    const double* S = ws + plan.soff[L];
+    long ld = plan.rows[L];
+    long r0 = (long)kNB * idxs[L - 1];
+    for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+      int r = e & 31, c = e >> 5;
+      sm.B[r * 33 + c] = __ldcg(S + r0 + r + (long)c * ld);
+    }
+    __syncthreads();
+    mul32(sm.B, sm.M, sm.T);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+      int r = e & 31, c = e >> 5;
+      sm.M[r * 33 + c] = sm.T[r * 33 + c];
+    }
+    __syncthreads();
+  }
+}
+
+// mode 0: write the explicit thin Q into A (evd_tsqr).
+// mode 1: write Y (into Yout), W (into Wout), and optionally the band panel
+//         (R over zeros) into Aband (sy2sb).
+__global__ void __launch_bounds__(kThreads)
+    tsqr_finish_kernel(const TsqrPlan plan, const double* ws, double* A, long lda, int mode,
+                       double* Yout, long ldy, double* Wout, long ldw, const double* Rin,
+                       long ldr, double* Aband, long ldband) {
+  extern __shared__ double dsm[];
+  __shared__ FinishSmem sm;
+  double* Qs = dsm;                   // 128 x 33 : tile rows of Q (then Y)
+  double* Ws = dsm + kTile * 33;      // 128 x 33 : W rows
+  const int t = blockIdx.x;
+  const int r0 = t * kTile;
+  const int mm = min(kTile, plan.m - r0);
+
+  // tile rows of Q = Qleaf_t * M_t
+  path_product(plan, ws, t, sm);
+  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
+    int r = e & (kTile - 1), c = e >> 7;
+    double s = 0.0;
+    if (r < mm) {
+      const double* qr = A + (long)(r0 + r);
+#pragma unroll 8
+      for (int k = 0; k < kNB; ++k) s = fma(__ldcg(qr + (long)k * lda), sm.M[k * 33 + c], s);
+    }
+    Qs[r * 33 + c] = s;
+  }
+  __syncthreads();
+
+  if (mode == 0) {
+    for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
+      int r = e & (kTile - 1), c = e >> 7;
+      if (r < mm) A[(long)(r0 + r) + (long)c * lda] = Qs[r * 33 + c];
+    }
+    return;
+  }
+
+  // LU of (I - Qtop), Qtop = Qleaf_0[0:32] * M_0 (recomputed by every CTA)
+  if (t != 0) path_product(plan, ws, 0, sm);
+  {
+    const double* q0 = ws + plan.qtop_off;
+    if (t == 0) {
+      for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+        int r = e & 31, c = e >> 5;
+        sm.LU[r * 33 + c] = ((r == c) ? 1.0 : 0.0) - Qs[r * 33 + c];
+      }
+    } else {
+      for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
+        int r = e & 31, c = e >> 5;
+        double s = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < kNB; ++k) s = fma(__ldcg(q0 + r + k * kNB), sm.M[k * 33 + c], s);
+        sm.LU[r * 33 + c] = ((r == c) ? 1.0 : 0.0) - s;
+      }
+    }
+  }
+  __syncthreads();
+  // unpivoted LU in place (one warp; lane = row)
+  if (threadIdx.x < 32) {
+    const int r = threadIdx.x;
+    for (int k = 0; k < kNB; ++k) {
+      double piv = sm.LU[k * 33 + k];
+      __syncwarp();
+      if (r > k) {
+        double l = sm.LU[r * 33 + k] / piv;
+        sm.LU[r * 33 + k] = l;
+        for (int c = k + 1; c < kNB; ++c) sm.LU[r * 33 + c] = fma(-l, sm.LU[k * 33 + c], sm.LU[r * 33 + c]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+
+  // per row: iq = e_gr - q ;  even thread -> Y row, odd thread -> W row
+  const int row = threadIdx.x >> 1;
+  const bool doW = threadIdx.x & 1;
+  double x[kNB];
+  if (row < mm) {
+    const int gr = r0 + row;
+#pragma unroll
+    for (int h = 0; h < kNB; ++h) x[h] = ((gr == h) ? 1.0 : 0.0) - Qs[row * 33 + h];
+    if (!doW) {
+      if (gr < kNB) {
+#pragma unroll
+        for (int h = 0; h < kNB; ++h) x[h] = (h < gr) ? sm.LU[gr * 33 + h] : ((h == gr) ? 1.0 : 0.0);
+      } else {
+        // y U = iq  (U upper, non-unit)
+#pragma unroll
+        for (int h = 0; h < kNB; ++h) {
+          double s = x[h];
+#pragma unroll
+          for (int k = 0; k < h; ++k) s = fma(-x[k], sm.LU[k * 33 + h], s);
+          x[h] = s / sm.LU[h * 33 + h];
+        }
+      }
+    } else {
+      // w L1^T = iq  (L1 unit lower): w_j = iq_j - sum_{k<j} L1[j,k] w_k
+#pragma unroll
+      for (int h = 0; h < kNB; ++h) {
+        double s = x[h];
+#pragma unroll
+        for (int k = 0; k < h; ++k) s = fma(-sm.LU[h * 33 + k], x[k], s);
+        x[h] = s;
+      }
+    }
+  }
+  __syncthreads();
+  if (row < mm) {
+    double* dst = doW ? Ws : Qs;
+#pragma unroll
+    for (int h = 0; h < kNB; ++h) dst[row * 33 + h] = x[h];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
+    int r = e & (kTile - 1), c = e >> 7;
+    if (r < mm) {
+      long gr = r0 + r;
+      Yout[gr + (long)c * ldy] = Qs[r * 33 + c];
+      Wout[gr + (long)c * ldw] = Ws[r * 33 + c];
+      if (Aband) {
+        double v = 0.0;
+        if (gr < kNB && c >= gr) v = __ldcg(Rin + gr + (long)c * ldr);
+        Aband[gr + (long)c * ldband] = v;
+      }
+    }
+  }
+}
+
+constexpr size_t kFinishDyn = 2 * kTile * 33 * sizeof(double);
+
+int finish_attr() {
+  static bool done = false;
+  if (!done) {
+    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_finish_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kFinishDyn));
+    done = true;
+  }
+  return EVD_SUCCESS;
+}
+
+}  // namespace
+
+long panel_qr_ws_doubles(long m) { return make_plan(m).total; }
+
+int panel_qr_check(long m, long n, long lda) {
+  if (n != kNB || m < kNB || (m % kNB) != 0 || lda < m) return EVD_ERR_INVALID_ARG;
+  if (m > (1L << 30)) return EVD_ERR_INVALID_ARG;
+  return EVD_SUCCESS;
+}
+
+int panel_counters_reset(long m, double* ws, cudaStream_t st) {
+  TsqrPlan plan = make_plan(m);
+  if (plan.ncnt > 0)
+    EVD_CUDA_TRY(cudaMemsetAsync(ws + plan.cnt_off, 0, sizeof(int) * plan.ncnt, st));
+  return EVD_SUCCESS;
+}
+
+int panel_qr_launch(long m, double* A, long lda, double* ws, int mode, double* Yout, long ldy,
+                    double* Wout, long ldw, double* R, long ldr, double* Aband, long ldband,
+                    cudaStream_t st) {
+  TsqrPlan plan = make_plan(m);
+  if (plan.nlev >= kMaxLevels) return EVD_ERR_INVALID_ARG;
+  tsqr_up_kernel<<<plan.T[0], kThreads, 0, st>>>(plan, A, lda, ws, R, ldr);
+  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_TRY(finish_attr());
+  tsqr_finish_kernel<<<plan.T[0], kThreads, kFinishDyn, st>>>(plan, ws, A, lda, mode, Yout, ldy,
+                                                              Wout, ldw, R, ldr, Aband, ldband);
+  EVD_CUDA_TRY(cudaGetLastError());
+  return EVD_SUCCESS;
+}
+
+}  // namespace evd
+
+extern "C" long evd_panel_qr_work_size(long m, long n) {
+  if (evd::panel_qr_check(m, n, m) != EVD_SUCCESS) return 0;
+  return evd::panel_qr_ws_doubles(m);
+}
+
+extern "C" int evd_tsqr(long m, long n, double* A, long lda, double* R, long ldr, double* work,
+                        long lwork, cudaStream_t stream) {
+  EVD_TRY(evd::panel_qr_check(m, n, lda));
+  if (!A || !R || !work || ldr < n) return EVD_ERR_INVALID_ARG;
+  if (lwork < evd::panel_qr_ws_doubles(m)) return EVD_ERR_WORKSPACE;
+  EVD_TRY(evd::panel_counters_reset(m, work, stream));
+  return evd::panel_qr_launch(m, A, lda, work, 0, nullptr, 0, nullptr, 0, R, ldr, nullptr, 0,
+                              stream);
+}
+
+extern "C" int evd_panel_qr(long m, long n, double* A, long lda, double* W, long ldw, double* R,
+                            long ldr, double* work, long lwork, cudaStream_t stream) {
+  EVD_TRY(evd::panel_qr_check(m, n, lda));
+  if (!A || !W || !R || !work || ldr < n || ldw < m) return EVD_ERR_INVALID_ARG;
+  if (lwork < evd::panel_qr_ws_doubles(m)) return EVD_ERR_WORKSPACE;
+  EVD_TRY(evd::panel_counters_reset(m, work, stream));
+  return evd::panel_qr_launch(m, A, lda, work, 1, A, lda, W, ldw, R, ldr, nullptr, 0, stream);
+}

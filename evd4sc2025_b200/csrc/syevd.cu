@@ -1,0 +1,165 @@
+// Whole two-stage eigensolver (plain FP64): the pipeline of the reference
+// driver `myEVD n b nb` (src/EVD/myEVD.cu:251-706) behind one C entry point.
+//
+//   A -> [sy2sb] band B, W, Y -> [band pack + bulge chasing] T = (d, e), U
+//     -> [device D&C] T = Z diag(w) Z^T
+//     -> X = Q2 Z [stage-2 back transformation, reflectors from U]
+//     -> X = Q1 X [stage-1 back transformation, slab-merged WY from W, Y]
+//
+// Differences from the reference driver: the tridiagonal solve runs on the GPU
+// (the reference copies T to the host for MKL dstedc and overlaps it with the
+// back transformation on a second host thread); Q1 and Q2 are applied to the
+// eigenvectors directly instead of forming Q = Q2^T Q1^T explicitly and
+// multiplying by Z in a final GEMM (saves 4n^3 flops); one process can call it
+// any number of times (the reference's chasing kernel keeps a global flag that
+// makes a second call return early).
+#include <vector>
+
+#include "common.cuh"
+#include "gemm_f64.cuh"
+
+namespace evd {
+
+long sy2sb_ws_doubles(long M, long b, long nb);
+int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, long ldA,
+          double* dW, long ldW, double* dY, long ldY, double* dZ, long ldZ, double* dR, long ldR,
+          double* work, long lwork, cudaStream_t st);
+int copy_matrix(long m, long n, const double* src, long lds, double* dst, long ldd,
+                cudaStream_t st);
+int band_pack(long n, long b, const double* dA, long ldA, double* dSub, long ldSub,
+              cudaStream_t st);
+long chase_iwork_ints(long n);
+int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU, double* d,
+                      double* e, int* iwork, cudaStream_t st);
+long stedc_ws_doubles(long n);
+long stedc_ws_ints(long n);
+int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
+          long liwork, cudaStream_t st);
+int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
+             cudaStream_t st);
+long sbr_back_ws_doubles(long n, long b, long nk);
+int wy_merge_slabs(long n, long b, long nk, long ncolsWY, double* dW, long ldW, const double* dY,
+                   long ldY, double* work, cudaStream_t st);
+int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const double* dY,
+                    long ldY, double* X, long ldX, long ncols, double* work, size_t work_n,
+                    cudaStream_t st);
+
+namespace {
+
+struct SyevdLayout {
+  long nb_eff;
+  size_t oOA, oA, oW, oY, oZ, oR, oS, oSub, oU, oD, oE, oStedc, oSbr, end_d;  // doubles
+  size_t oIchase, oIstedc, end_i;                                          // ints
+  size_t bytes;
+};
+
+SyevdLayout layout(long n, long b, long nb) {
+  SyevdLayout L{};
+  auto al = [](size_t x) { return (x + 31) / 32 * 32; };
+  size_t o = 0;
+  const size_t nn = (size_t)n * n;
+  L.oOA = o; o = al(o + nn);
+  L.oA = o; o = al(o + nn);
+  L.oW = o; o = al(o + nn);
+  L.oY = o; o = al(o + nn);
+  L.oZ = o; o = al(o + (size_t)n * nb);
+  L.oR = o; o = al(o + (size_t)n * nb);
+  L.oS = o; o = al(o + sy2sb_ws_doubles(n, b, nb));
+  L.oSub = o; o = al(o + (size_t)2 * b * n);
+  L.oU = o; o = al(o + nn);
+  L.oD = o; o = al(o + n);
+  L.oE = o; o = al(o + n);
+  L.oStedc = o; o = al(o + stedc_ws_doubles(n));
+  L.oSbr = o; o = al(o + sbr_back_ws_doubles(n, b, nb));
+  L.end_d = o;
+  size_t q = 0;
+  L.oIchase = q; q = al(q + chase_iwork_ints(n));
+  L.oIstedc = q; q = al(q + stedc_ws_ints(n));
+  L.end_i = q;
+  L.bytes = L.end_d * sizeof(double) + L.end_i * sizeof(int) + 256;
+  return L;
+}
+
+thread_local double g_timings[6] = {0, 0, 0, 0, 0, 0};
+
+}  // namespace
+
+int syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X, long ldX,
+          void* work, long lwork_bytes, int timed, cudaStream_t st) {
+  if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
+  long q = nb / b;
+  if (q & (q - 1)) return EVD_ERR_INVALID_ARG;  // slab merge needs nb = b * 2^k
+  if (lda < n || ldX < n || !A || !w || !X || !work) return EVD_ERR_INVALID_ARG;
+  SyevdLayout L = layout(n, b, nb);
+  if ((size_t)lwork_bytes < L.bytes) return EVD_ERR_WORKSPACE;
+  double* base = reinterpret_cast<double*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  int* ibase = reinterpret_cast<int*>(base + L.end_d);
+  double *OA = base + L.oOA, *dA = base + L.oA, *W = base + L.oW, *Y = base + L.oY,
+         *Z = base + L.oZ, *R = base + L.oR, *S = base + L.oS, *sub = base + L.oSub,
+         *U = base + L.oU, *d = base + L.oD, *e = base + L.oE, *SW = base + L.oStedc,
+         *SB = base + L.oSbr;
+  int* ich = ibase + L.oIchase;
+  int* ist = ibase + L.oIstedc;
+
+  cudaEvent_t ev[6];
+  if (timed) {
+    for (auto& x : ev) EVD_CUDA_TRY(cudaEventCreate(&x));
+    EVD_CUDA_TRY(cudaEventRecord(ev[0], st));
+  }
+  // ---- stage 1: full -> band ----
+  EVD_TRY(copy_matrix(n, n, A, lda, OA, n, st));
+  EVD_TRY(copy_matrix(n, n, A, lda, dA, n, st));
+  EVD_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * n * n, st));
+  EVD_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * n * n, st));
+  EVD_TRY(sy2sb(n, n, b, nb, OA, n, dA, n, W, n, Y, n, Z, n, R, n, S,
+                (long)sy2sb_ws_doubles(n, b, nb), st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[1], st));
+  // ---- stage 2: band -> tridiagonal ----
+  EVD_TRY(band_pack(n, b, dA, n, sub, 2 * b, st));
+  EVD_CUDA_TRY(cudaMemsetAsync(U, 0, sizeof(double) * n * n, st));
+  EVD_TRY(bulge_chase_async(n, b, sub, 2 * b, U, n, d, e, ich, st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[2], st));
+  // ---- tridiagonal D&C (eigenvectors straight into X) ----
+  EVD_TRY(stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[3], st));
+  // ---- back transformations ----
+  EVD_TRY(q2_apply(false, n, n, U, n, X, ldX, st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[4], st));
+  const long npcols = ((n - 1) / b) * b;
+  EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, st));
+  EVD_TRY(sbr_apply_slabs(n, b, nb, W, n, Y, n, X, ldX, n, SB,
+                          (size_t)sbr_back_ws_doubles(n, b, nb), st));
+  EVD_CUDA_TRY(cudaMemcpyAsync(w, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (timed) {
+    EVD_CUDA_TRY(cudaEventRecord(ev[5], st));
+    EVD_CUDA_TRY(cudaEventSynchronize(ev[5]));
+    float ms;
+    for (int i = 0; i < 5; ++i) {
+      EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      g_timings[i] = ms;
+    }
+    EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[5]));
+    g_timings[5] = ms;
+    for (auto& x : ev) cudaEventDestroy(x);
+  }
+  // chasing error word (bounded waits) is checked once at the end
+  return read_device_error(ich + n + 32, st);
+}
+
+size_t syevd_ws_bytes(long n, long b, long nb) { return layout(n, b, nb).bytes; }
+
+}  // namespace evd
+
+extern "C" long evd_syevd_work_size(long n, long b, long nb) {
+  if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return 0;
+  return (long)evd::syevd_ws_bytes(n, b, nb);
+}
+
+extern "C" void evd_syevd_last_timings(double out_ms[6]) {
+  for (int i = 0; i < 6; ++i) out_ms[i] = evd::g_timings[i];
+}
+
+extern "C" int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X,
+                         long ldX, void* work, long lwork_bytes, int timed, cudaStream_t stream) {
+  return evd::syevd(n, b, nb, A, lda, w, X, ldX, work, lwork_bytes, timed, stream);
+}

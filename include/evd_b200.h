@@ -1,0 +1,213 @@
+/*
+ * evd_b200.h — C ABI of the B200-native two-stage symmetric eigensolver.
+ *
+ * Every entry point is `extern "C"`, takes plain device pointers, 64-bit sizes
+ * and leading dimensions (column-major FP64, as the reference), and a CUDA
+ * stream (NULL = legacy default stream, which is what every reference routine
+ * uses).  Each returns an int status (EVD_SUCCESS or a negative EVD_ERR_*).
+ * No entry point allocates device memory unless its comment says so; the
+ * caller passes workspaces sized by the matching *_work_size query.
+ *
+ * The comment on each function names the reference interface it replaces
+ * (paths relative to the hansheng1001/EVD4SC2025 source tree).  The reference
+ * functions take cuBLAS/cuSOLVER handles; this library uses none, so the C++
+ * shims in evd_b200_compat.hpp accept and ignore them.
+ */
+#ifndef EVD_B200_H
+#define EVD_B200_H
+
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define EVD_SUCCESS 0
+#define EVD_ERR_INVALID_ARG (-1)   /* bad size / leading dimension / pointer     */
+#define EVD_ERR_CUDA (-2)          /* a CUDA runtime call failed                  */
+#define EVD_ERR_TIMEOUT (-3)       /* a bounded device-side wait ran out          */
+#define EVD_ERR_NO_CONVERGENCE (-4)/* an iterative solver did not converge        */
+#define EVD_ERR_WORKSPACE (-5)     /* workspace smaller than the size query says  */
+
+/* Human-readable text for a status code (static storage). */
+const char* evd_status_string(int status);
+
+/* Library version string, e.g. "evd_b200 0.1 sm_100a". */
+const char* evd_version(void);
+
+/* ---- FP64 GEMM / SYR2K building blocks --------------------------------- */
+
+/* C = alpha*op(A)*op(B) + beta*C, op = N ('n') or T ('t'); FP64 on DMMA.
+ * Replaces the cublasGemmEx / cublasDgemm (CUBLAS_COMPUTE_64F) calls the
+ * reference issues throughout (e.g. api/zy_zy_sy2sb.cu:134-347,
+ * src/EVD/myEVD.cu:227-232, :564). */
+int evd_dgemm(char transa, char transb, long m, long n, long k, double alpha,
+              const double* A, long lda, const double* B, long ldb, double beta,
+              double* C, long ldc, cudaStream_t stream);
+
+/* Strided-batched variant (replaces cublasGemmStridedBatchedEx in
+ * api/inc/TallShinnyQR.h:72-98 and src/EVD/myEVD.cu:151-206). */
+int evd_dgemm_strided_batched(char transa, char transb, long m, long n, long k,
+                              double alpha, const double* A, long lda, long strideA,
+                              const double* B, long ldb, long strideB, double beta,
+                              double* C, long ldc, long strideC, long batch,
+                              cudaStream_t stream);
+
+/* Lower-triangular SYR2K with mirrored upper triangle:
+ *   C = alpha*(A*B^T + B*A^T) + beta*C   (n x n, A and B n x k)
+ * then C(upper) = C(lower)^T.  Replaces tc_ozimmu_syr2k<double>
+ * (api/inc/tc_ozimmu_syr2k.h:6-18, api/TCblas/tc_ozimmu_syr2k.cu:631-681)
+ * followed by copyMatrixL2U (api/zy_zy_sy2sb.cu:436).  `nb` is accepted for
+ * signature parity and ignored (the tile schedule does not need it). */
+int evd_syr2k_lower_mirror(long n, long k, double alpha, const double* A, long lda,
+                           const double* B, long ldb, double beta, double* C, long ldc,
+                           long nb, cudaStream_t stream);
+
+/* ---- Stage 1: full -> band (ZY) ---------------------------------------- */
+
+/* Workspace (in doubles) needed by evd_tsqr / evd_panel_qr for an m x n panel. */
+long evd_panel_qr_work_size(long m, long n);
+
+/* Tall-skinny QR with explicit Q: A (m x n, n == 32) is overwritten by the
+ * explicit thin Q, R (n x n) receives the triangular factor.  Tiles of 128
+ * rows, reduction tree of fan-in 4, as hou_tsqr_panel<double,128,32>
+ * (api/inc/TallShinnyQR.h:9-133, util/inc/kernelQR.h:215-414).
+ * Requires (m % 128) % n == 0 like the reference (TallShinnyQR.h:37-41). */
+int evd_tsqr(long m, long n, double* A, long lda, double* R, long ldr,
+             double* work, long lwork, cudaStream_t stream);
+
+/* Panel QR in compact form Q = I - W*Y^T: A (m x n) is overwritten by Y
+ * (unit lower trapezoidal), W (m x n) and R (n x n) are written.  Replaces
+ * panelQR<double> (api/inc/PanelQR.h:7-18, api/panelQR.cu:20-246): TSQR,
+ * then the unpivoted LU of (I - Q) and W = (I - Q) * L1^{-T}. */
+int evd_panel_qr(long m, long n, double* A, long lda, double* W, long ldw, double* R,
+                 long ldr, double* work, long lwork, cudaStream_t stream);
+
+/* Workspace (doubles) for evd_sy2sb. */
+long evd_sy2sb_work_size(long M, long b, long nb);
+
+/* Full-to-band reduction with the ZY update.  Argument meaning as
+ * my_ZY_ZY_SBR_Vector<double> (api/inc/zy_zy_sy2sb.h:5-24,
+ * api/zy_zy_sy2sb.cu:24-486): dOriA holds the full symmetric matrix and is
+ * destroyed; dA receives the band matrix (lower band, R blocks); the W and Y
+ * factors of each b-wide panel are left at (i, i-b) of dW / dY; dZ (M x nb)
+ * and dR (M x nb) are scratch.  On return dA is symmetric (both triangles),
+ * as after the reference's copyMatrixL2U (src/EVD/myEVD.cu:346).
+ * Requires b == 32, M == N, M % nb == 0, nb % b == 0. */
+int evd_sy2sb(long M, long N, long b, long nb, double* dOriA, long ldOriA, double* dA,
+              long ldA, double* dW, long ldW, double* dY, long ldY, double* dZ, long ldZ,
+              double* dR, long ldR, double* work, long lwork, cudaStream_t stream);
+
+/* ---- Stage 2: band -> tridiagonal (bulge chasing) ----------------------- */
+
+/* Pack the lower band of dA into band storage sub(i + j*ldSub) = A(j+i, j),
+ * i < 2b, zero below the band (kernel_bugle_chasing_cpydA2dSubA,
+ * src/EVD/myEVD.cu:53-78). */
+int evd_band_pack(long n, long b, const double* dA, long ldA, double* dSub, long ldSub,
+                  cudaStream_t stream);
+
+/* Bytes of int scratch needed by evd_bulge_chase (progress flags + counters). */
+long evd_bulge_chase_iwork_size(long n);
+
+/* Band -> tridiagonal.  dSub is band storage (ldSub >= 2b) and is overwritten;
+ * every Householder vector (||u||^2 = 2) is written into dU column s (sweep s),
+ * 32-row segments starting at row s+1, exactly where chasing_kernel_one_timeV10
+ * writes them (util/inc/bugle_chasingV10.h:21-392, launched at
+ * src/EVD/myEVD.cu:383-439).  dU must have ldU >= n and is NOT cleared here
+ * (clear it first, as the reference does at src/EVD/myEVD.cu:413).  d (n) and
+ * e (n-1) receive the tridiagonal (kernel_bugle_chasing_cpydSubA2dA +
+ * cpyATr2Vector, src/EVD/myEVD.cu:105-123, :477-480).  iwork: evd_bulge_chase_iwork_size
+ * bytes of device memory.  b must be 32. */
+int evd_bulge_chase(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
+                    double* d, double* e, int* iwork, cudaStream_t stream);
+
+/* ---- Tridiagonal eigensolver (device divide and conquer) ---------------- */
+
+long evd_stedc_work_size(long n);   /* doubles */
+long evd_stedc_iwork_size(long n);  /* ints    */
+
+/* All eigenvalues (ascending, into d) and eigenvectors (Z, n x n) of the
+ * symmetric tridiagonal (d, e).  Replaces the host LAPACKE_dstedc('I') call of
+ * the reference driver (src/EVD/myEVD.cu:529) with a device divide and
+ * conquer.  d and e are device arrays; e is destroyed. */
+int evd_stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork,
+              int* iwork, long liwork, cudaStream_t stream);
+
+/* ---- Back transformations ----------------------------------------------- */
+
+/* Q <- Q2^T * Q, Q2 = product of the chasing reflectors stored in U (generation
+ * order).  Same signature and meaning as my_BC_back_trans_v8_10_noBandU
+ * (api/inc/BC_backTrans.h:3, api/BC_backTransV8_10_noBandU.cu:234-313).  Q has
+ * n rows (rows >= n are neither read nor written, so no padding is needed);
+ * U is the chasing output (ldU >= n).  Returns 0 on success. */
+int evd_bc_back(double* Q, long ldQ, const double* U, long ldU, long n, int b,
+                cudaStream_t stream);
+
+/* X <- Q2 * X for an n x ncols block X (the eigenvector direction: reflectors
+ * applied in reverse generation order). */
+int evd_bc_back_apply(long n, long ncols, const double* U, long ldU, double* X, long ldX,
+                      int b, cudaStream_t stream);
+
+/* Merge the b-wide compact-WY slides of an M x N block into one compact WY:
+ * W[:, i-b:i] -= W[:, 0:i-b] * (Y[:, 0:i-b]^T * W[:, i-b:i]) for i = 2b..N.
+ * Same as computerWYFromSlide (api/inc/computerWYFromSlide.h:4,
+ * api/computerWYFromSlide.cu:5-25); work >= M*N doubles is unused here but kept
+ * for signature parity (pass NULL to skip). */
+int evd_wy_from_slide(long M, long N, long slideWidth, double* dW, long ldW,
+                      const double* dY, long ldY, double* work, cudaStream_t stream);
+
+/* Q = I - W*Y^T (M x M), as computerQFromWY (api/inc/computerQFromWY.h:4,
+ * api/computerQFromWY.cu:5-17). */
+int evd_q_from_wy(long M, long N, double* dQ, long ldQ, const double* dW, long ldW,
+                  const double* dY, long ldY, cudaStream_t stream);
+
+/* Workspace (doubles) for evd_sbr_back. */
+long evd_sbr_back_work_size(long n, long b, long nk);
+
+/* X <- Q1 * X with Q1 = prod_p (I - W_p Y_p^T) over the b-wide panels left by
+ * evd_sy2sb in dW/dY (panel p at rows/cols (p+1)b.., p*b..).  Panels are merged
+ * into nk-wide slabs first (the inline merge of my_SBRBack_BCBack,
+ * src/EVD/myEVD.cu:148-207; dW is overwritten by the merged W), then each slab
+ * is applied to X.  The reference instead forms Q1 from I
+ * (src/EVD/myEVD.cu:213-233) and multiplies by Z afterwards (:564). */
+int evd_sbr_back(long n, long b, long nk, double* dW, long ldW, const double* dY,
+                 long ldY, double* X, long ldX, long ncols, double* work, long lwork,
+                 cudaStream_t stream);
+
+/* ---- Metrics (a13) --------------------------------------------------------- */
+
+/* result[0] = ||A^T B - I||_F / M  (checkOrthogonality,
+ * util/tool/checkMetric.cu:5-24, which prints instead of returning).
+ * work >= M*M doubles. */
+int evd_check_orthogonality(long M, long N, const double* dA, long ldA, const double* dB,
+                            long ldB, double* work, double* result, cudaStream_t stream);
+
+/* result[0] = ||A X - X diag(w)||_F / (n ||A||_F), result[1] = ||X^T X - I||_F / n.
+ * work >= 2*n*n doubles. */
+int evd_check_eig(long n, const double* A, long lda, const double* w, const double* X,
+                  long ldX, double* work, double* result, cudaStream_t stream);
+
+/* ---- Whole solver ------------------------------------------------------- */
+
+/* Bytes of device workspace for evd_syevd. */
+long evd_syevd_work_size(long n, long b, long nb);
+
+/* Stage timings (milliseconds, CUDA events) of the last evd_syevd call on this
+ * host thread: [0] sy2sb, [1] bulge chasing, [2] tridiagonal D&C,
+ * [3] stage-2 back transformation, [4] stage-1 back transformation, [5] total. */
+void evd_syevd_last_timings(double out_ms[6]);
+
+/* Eigenvalues w (ascending, device, n) and eigenvectors X (n x n, device) of the
+ * symmetric A (device, full storage; A is not modified).  The plain-FP64
+ * two-stage pipeline of the reference driver `myEVD n b nb`
+ * (src/EVD/myEVD.cu:251-706): sy2sb -> bulge chasing -> tridiagonal D&C ->
+ * stage-2 then stage-1 back transformation.  work: evd_syevd_work_size bytes. */
+int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X,
+              long ldX, void* work, long lwork_bytes, int timed, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EVD_B200_H */

@@ -1,0 +1,69 @@
+"""Whole plain-FP64 pipeline (evd_syevd) vs LAPACK dsyevd and the oracle pipeline."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import algos as O
+
+pytestmark = pytest.mark.gpu
+
+# eigenvalues to 1e-12 relative to ||A||, residual and
+# orthogonality below 1e-13 (normalised by n, as the reference's checkMetric)
+TOL_VAL = 1e-12
+TOL_RES = 1e-13
+TOL_ORT = 1e-13
+
+
+def _run(cuda, evdlib, A, nb):
+    n = A.shape[0]
+    Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
+    w, X = evdlib.syevd(Ad, 32, nb)
+    res, orth = evdlib.check_eig(Ad, w, X)
+    torch.cuda.synchronize()
+    return w.cpu().numpy(), X.cpu().numpy(), res, orth
+
+
+@pytest.mark.parametrize("n,nb", [(64, 32), (256, 64), (1024, 256), (1024, 1024), (2048, 1024),
+                                  (4096, 1024)])
+def test_syevd_gaussian(cuda, evdlib, n, nb):
+    A = O.sym_gaussian(n, seed=2024 + n)
+    w, X, res, orth = _run(cuda, evdlib, A, nb)
+    w_ref = np.linalg.eigvalsh(A)
+    nA = np.linalg.norm(A, 2)
+    assert np.abs(w - w_ref).max() <= TOL_VAL * nA
+    assert res <= TOL_RES and orth <= TOL_ORT
+    # CPU-side residual for an independent check
+    assert O.residual(A, w, X) <= TOL_RES
+
+
+def test_syevd_matches_oracle_pipeline(cuda, evdlib):
+    n, nb = 512, 256
+    A = O.sym_gaussian(n, seed=77)
+    w, X, res, orth = _run(cuda, evdlib, A, nb)
+    w_o, X_o, _ = O.syevd_two_stage(A, 32, nb)
+    assert np.abs(w - w_o).max() <= TOL_VAL * np.linalg.norm(A, 2)
+    # eigenvectors agree up to sign (simple spectrum)
+    s = np.sign(np.sum(X * X_o, axis=0))
+    assert np.abs(X - X_o * s).max() <= 1e-9
+
+
+@pytest.mark.parametrize("kind", ["geometric", "uniform", "clustered", "geometric1e10"])
+def test_syevd_known_spectrum(cuda, evdlib, kind):
+    n, nb = 1024, 256
+    A, lam = O.known_spectrum_matrix(kind, n, seed=5)
+    w, X, res, orth = _run(cuda, evdlib, A, nb)
+    # lambda is known up to the error of forming A (~sqrt(n) eps ||A||)
+    assert np.abs(w - lam).max() <= 1e-12 * np.abs(lam).max() * 4
+    assert res <= TOL_RES and orth <= TOL_ORT
+
+
+def test_syevd_repeatable_and_timed(cuda, evdlib):
+    n = 1024
+    A = evdlib.to_cm(torch.from_numpy(O.sym_gaussian(n, 1)), device=cuda)
+    ws = evdlib.Workspace(n, 32, 256, device=cuda)
+    w1, X1 = evdlib.syevd(A, 32, 256, ws=ws, timed=True)
+    t = evdlib.last_timings()
+    w2, X2 = evdlib.syevd(A, 32, 256, ws=ws)
+    torch.cuda.synchronize()
+    assert torch.equal(w1, w2) and torch.equal(X1, X2)  # deterministic
+    assert t["total"] > 0 and all(v >= 0 for v in t.values())
