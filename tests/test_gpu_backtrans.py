@@ -35,17 +35,15 @@ def test_q2_apply_matches_oracle(cuda, evdlib, n, ncols, forward):
 
 
 def _fwd(evdlib, Xd, Ud):
-    # forward direction on a non-square block: Q2^T X via Q2^T = (Q2)^T applied to columns
-    import ctypes as C
-    from evd4sc2025_b200._native import call
-    # evd_bc_back is square-only (reference signature); transpose trick through the
-    # reverse kernel: Q2^T X = (X^T Q2)^T is not available, so use the square API on a
-    # padded copy.
+    """Q2^T X for any column count through the square reference entry point:
+    process X in chunks of at most n columns padded into an n x n block."""
     n, k = Xd.shape
-    P = evdlib.zeros_cm(n, n, device=Xd.device)
-    P[:, :k] = Xd
-    evdlib.bc_back(P, Ud)
-    Xd.copy_(P[:, :k])
+    for c0 in range(0, k, n):
+        c1 = min(k, c0 + n)
+        P = evdlib.zeros_cm(n, n, device=Xd.device)
+        P[:, : c1 - c0] = Xd[:, c0:c1]
+        evdlib.bc_back(P, Ud)
+        Xd[:, c0:c1] = P[:, : c1 - c0]
 
 
 def test_bc_back_reference_semantics(cuda, evdlib):
