@@ -1,0 +1,339 @@
+#!/usr/bin/env python3
+"""Benchmark: seconds per n=16384 FP64 symmetric EVD (all eigenpairs) on B200.
+
+    python bench.py --gpus N --steps K --warmup W [--impl ours|reference] [--n 16384]
+
+One step = one full eigendecomposition (eigenvalues + eigenvectors) of a seeded
+symmetrised Gaussian A = (G + G^T)/2, n = 16384, b = 32, nb = 1024 (the plain
+FP64 two-stage configuration of the reference's `myEVD 16384 32 1024`).
+
+* value:   device time per EVD with A already resident in HBM (CUDA events on
+           the solver stream, W warm-up steps, K timed steps, max over ranks);
+           whole-job seconds per EVD = step time / N GPUs (independent replicas).
+* e2e:     the same through the public API with HOST buffers: pinned H2D of A,
+           the solve, D2H of eigenvalues and eigenvectors, inside the timed
+           region.
+* Every matrix is 2 GiB (> 126 MB L2), so no L2 flush is needed between steps.
+* cpu_baseline: LAPACK dsyevd (scipy/OpenBLAS, all host cores) on a bounded
+  sample (n=4096, or 8192 when fast enough), scaled by n^3 to n=16384.
+* --impl reference: the reference's own GPU build (oracle/_ref/ref_driver,
+  compiled from the reference sources; host dstedc via scipy's OpenBLAS) on
+  the same n/b/nb, timed by its own driver; rank 0 only.
+Multi-GPU: replicas only (a single EVD is not sharded; no collectives on the
+data path).  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "s per n=16384 EVD (resid<=1e-13), plain FP64 two-stage"
+UNIT = "s/EVD"
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# -------------------------------------------------------------- CPU baseline
+def cpu_baseline(n_target: int) -> dict:
+    """LAPACK dsyevd on the host (the oracle's CPU checker), bounded sample."""
+    import numpy as np
+    import scipy.linalg as sla
+    cores = os.cpu_count() or 1
+    sample_n, t = None, None
+    for n in (4096, 8192):
+        rng = np.random.default_rng(0)
+        G = rng.standard_normal((n, n))
+        A = 0.5 * (G + G.T)
+        t0 = time.perf_counter()
+        sla.eigh(A, driver="evd", overwrite_a=True, check_finite=False)
+        dt = time.perf_counter() - t0
+        sample_n, t = n, dt
+        if dt * 8 > 25.0:   # the next size would exceed the ~30 s budget
+            break
+    scale = (n_target / sample_n) ** 3
+    return {"value": t * scale, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"LAPACK dsyevd (scipy OpenBLAS, {cores} threads) n={sample_n}: "
+                      f"{t:.3f} s, scaled by (n/{sample_n})^3"}
+
+
+# ------------------------------------------------------------ reference arm
+def run_reference(args) -> int:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    drv = ROOT / "oracle" / "_ref" / "ref_driver"
+    base = {"metric": METRIC, "unit": UNIT, "impl": "reference", "higher_is_better": False}
+    if not drv.exists():
+        print(json.dumps({**base, "unavailable": "oracle/_ref/ref_driver not built "
+                                                  "(make -C oracle needs the reference sources)"}))
+        return 0
+    reps = args.warmup + args.steps
+    t0 = time.perf_counter()
+    res = subprocess.run([str(drv), str(args.n), "32", str(args.nb), "-", "-", str(reps)],
+                         capture_output=True, text=True, timeout=3600)
+    wall = time.perf_counter() - t0
+    recs = []
+    for ln in res.stdout.splitlines():
+        ln = ln.strip()
+        if ln.startswith("{") and ln.endswith("}"):
+            try:
+                recs.append(json.loads(ln))
+            except json.JSONDecodeError:
+                pass
+    if res.returncode != 0 or len(recs) < reps:
+        print(json.dumps({**base, "unavailable": f"reference driver failed rc={res.returncode}: "
+                                                  f"{res.stderr.strip()[-200:]}"}))
+        return 0
+    timed = recs[args.warmup:]
+    ms = max(r["total_ms"] for r in timed)
+    mean_ms = sum(r["total_ms"] for r in timed) / len(timed)
+    value = mean_ms / 1000.0
+    stages = {k: round(sum(r[k] for r in timed) / len(timed), 2)
+              for k in ("sy2sb_ms", "chase_ms", "dstedc_host_ms", "back_ms", "dc_back_overlap_ms",
+                        "final_gemm_ms")}
+    cores = os.cpu_count() or 1
+    line = {
+        **base, "value": value, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mean_ms, "max_ms_per_step": ms, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (reference cuRAND U(0,1], seed 3000, symmetrised)",
+        "config": {"workload": f"plain FP64 two-stage EVD n={args.n} b=32 nb={args.nb}",
+                   "n": args.n, "b": 32, "nb": args.nb, "parallelism": "replicas"},
+        "stages_ms": stages,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "reference GPU build (sm_100a compile of its sources) with "
+                                   "host dstedc (OpenBLAS) overlapped, full n per step"},
+        "wall_s": wall,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args) -> int:
+    import torch
+    import torch.distributed as dist
+
+    import evd4sc2025_b200 as evd
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, b, nb = args.n, 32, args.nb
+    stream = torch.cuda.Stream(device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device=dev).manual_seed(1234 + rank)
+        G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
+        A = evd.empty_cm(n, n, device=dev)
+        A.copy_(0.5 * (G + G.t()))
+        del G
+        ws = evd.Workspace(n, b, nb, device=dev)
+        w = torch.empty(n, dtype=torch.float64, device=dev)
+        X = evd.empty_cm(n, n, device=dev)
+        launches0 = evd.lib().evd_launch_count()
+        evd.syevd(A, b, nb, ws=ws, w=w, X=X, stream=stream)
+        launches_per_step = evd.lib().evd_launch_count() - launches0
+        for _ in range(max(0, args.warmup - 1)):
+            evd.syevd(A, b, nb, ws=ws, w=w, X=X, stream=stream)
+        stream.synchronize()
+
+    # ---- device-timed region: A resident ----
+    barrier()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    stage_sum = {}
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            evd.syevd(A, b, nb, ws=ws, w=w, X=X, timed=True, stream=stream)
+            for k, v in evd.last_timings().items():
+                stage_sum[k] = stage_sum.get(k, 0.0) + v
+        e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    stages = {k: v / args.steps for k, v in stage_sum.items()}
+    # note: timed=True inserts CUDA events between stages only (no sync inside a stage)
+
+    # ---- accuracy of the last result ----
+    with torch.cuda.stream(stream):
+        resid, orth = evd.check_eig(A, w, X, stream=stream)
+
+    # ---- e2e through the public API with host buffers ----
+    A_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    A_h.copy_(A.t())  # column-major bytes of A as a row-major (n, n) host array (A symmetric)
+    w_h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    X_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    A_d = evd.empty_cm(n, n, device=dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        f0.record(stream)
+        for _ in range(e2e_steps):
+            A_d.t().copy_(A_h, non_blocking=True)
+            evd.syevd(A_d, b, nb, ws=ws, w=w, X=X, stream=stream)
+            w_h.copy_(w, non_blocking=True)
+            X_h.copy_(X.t(), non_blocking=True)
+        f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te.item())
+
+    # ---- roofline of the dominant kernel ----
+    fp64_peak = evd.fp64_peak_tflops()
+    flops_total = 16.0 / 3.0 * n ** 3
+    stage_flops = {"sy2sb": 4.0 / 3.0 * n ** 3, "bc_back": 2.0 * n ** 3, "sbr_back": 2.0 * n ** 3}
+    dom = max(("sy2sb", "bulge_chasing", "tridiagonal_dc", "bc_back", "sbr_back"),
+              key=lambda k: stages.get(k, 0.0))
+    # the stage-2 back transformation is one kernel launch (q2_apply_kernel)
+    bc_ms = stages.get("bc_back", float("nan"))
+    achieved = stage_flops["bc_back"] / (bc_ms * 1e-3) / 1e12
+    roofline = {"kernel": "q2_apply_kernel (stage-2 back transformation, one launch)",
+                "bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": None,
+                "peak_source": "FP64 DMMA peak measured live by evd_fp64_peak_probe "
+                               "(MEASURED_PEAKS.json has no FP64 figure)",
+                "dominant_stage": dom,
+                "pipeline": {"flops_per_evd": flops_total,
+                             "achieved_tflops": flops_total / (ms * 1e-3) / 1e12,
+                             "frac": flops_total / (ms * 1e-3) / 1e12 / fp64_peak}}
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    cpu = cpu_baseline(n) if not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": ms_max / 1000.0 / world, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded symmetrised Gaussian A=(G+G^T)/2 (torch Philox seed 1234+rank)",
+        "config": {"workload": f"plain FP64 two-stage EVD n={n} b={b} nb={nb}", "n": n, "b": b,
+                   "nb": nb, "parallelism": f"replicas x{world}",
+                   "l2": "inputs 2 GiB > 126 MB L2 (no flush needed)"},
+        "stages_ms": {k: round(v, 3) for k, v in stages.items()},
+        "accuracy": {"resid": resid, "orth": orth, "resid_ok": resid <= 1e-13,
+                     "orth_ok": orth <= 1e-13},
+        "e2e": {"value": e2e_ms / 1000.0 / world, "unit": UNIT,
+                "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * 8 + n * n * 8},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roofline,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=16384)
+    ap.add_argument("--nb", type=int, default=1024)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU LAPACK baseline")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = max(args.warmup, 1)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -363,6 +363,13 @@ def syevd(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | None = N
 myEVD = syevd
 
 
+def fp64_peak_tflops(stream=None) -> float:
+    """Measured FP64 DMMA peak of this GPU (TFLOP/s)."""
+    out = (C.c_double * 1)()
+    call("evd_fp64_peak_probe", out, _stream(stream))
+    return float(out[0])
+
+
 def last_timings() -> dict:
     """Stage times (ms) of the last timed syevd call on this thread."""
     out = (C.c_double * 6)()

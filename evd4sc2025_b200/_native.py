@@ -21,6 +21,8 @@ _c = C.c_char
 SIGNATURES = {
     "evd_status_string": (C.c_char_p, [_i]),
     "evd_version": (C.c_char_p, []),
+    "evd_launch_count": (_l, []),
+    "evd_fp64_peak_probe": (_i, [_p, _p]),
     "evd_dgemm": (_i, [_c, _c, _l, _l, _l, _d, _p, _l, _p, _l, _d, _p, _l, _p]),
     "evd_dgemm_strided_batched": (_i, [_c, _c, _l, _l, _l, _d, _p, _l, _l, _p, _l, _l, _d,
                                        _p, _l, _l, _l, _p]),

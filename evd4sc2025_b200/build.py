@@ -3,8 +3,8 @@
 Every ``csrc/*.cu`` file is compiled with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`` into an object
 under ``_build/`` and linked into ``evd4sc2025_b200/libevd_b200.so`` next to
-this file (in-tree, so it travels with the source tree).  ``csrc/myEVD.cpp``
-is linked against it into ``evd4sc2025_b200/bin/myEVD``.
+this file (in-tree, so it travels with the source tree).
+``cli/myEVD.cu`` is linked against it into ``evd4sc2025_b200/bin/myEVD``.
 
 Usage: ``python -m evd4sc2025_b200.build [-j N] [--force]``.
 """
@@ -68,12 +68,12 @@ def build(jobs: int = 8, force: bool = False, verbose: bool = False) -> pathlib.
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
         if verbose:
             print(f"linked {LIB}")
-    cli_src = CSRC / "myEVD.cpp"
+    cli_src = PKG / "cli" / "myEVD.cu"
     if cli_src.exists():
         BIN.parent.mkdir(exist_ok=True)
         if force or not BIN.exists() or BIN.stat().st_mtime < max(
                 LIB.stat().st_mtime, cli_src.stat().st_mtime):
-            cmd = [_nvcc(), "-O2", "-std=c++17", "-I", str(INCLUDE), str(cli_src),
+            cmd = [_nvcc(), *ARCH, "-O2", "-std=c++17", "-I", str(INCLUDE), str(cli_src),
                    "-o", str(BIN), "-L", str(PKG), "-levd_b200",
                    "-Xlinker", "-rpath,$ORIGIN/.."]
             res = subprocess.run(cmd, capture_output=True, text=True)

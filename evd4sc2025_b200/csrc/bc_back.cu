@@ -232,7 +232,7 @@ int launch_q2(long n, long ncols, const double* U, long ldU, double* X, long ldX
   }
   int grid = ceil_div_i(ncols, kWarps * kCols);
   q2_apply_kernel<FWD><<<grid, kThreadsBC, kBCSmem, st>>>((int)n, (int)ncols, U, ldU, X, ldX);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 

@@ -8,23 +8,36 @@
 // where B1 is the block left of the diagonal block S2 (rows r..r+b-1) and B1'
 // the bulge block below S2.  u is stored into U(r:r+b, s).
 //
-// B200 design (not the reference's): instead of one 1024-thread CTA per sweep
-// with a grid.sync() after every step, each sweep is owned by ONE warp that
-// keeps B1/S2/B1' in a private shared-memory window, and sweeps are pipelined
-// through point-to-point progress flags (acquire/release at gpu scope).
-// Workers take sweeps from an atomic ticket, so the sweep a warp waits on was
-// taken earlier by a warp that is already running: no co-residency
-// requirement, no cooperative launch.  The dependency rule is the reference's
-// (step at opRow r may run once the previous sweep has published
-// prog >= r + 2b, :81).  Every wait is bounded in time; on timeout the kernel
-// records an error word and all workers drain, nothing spins forever.
+// B200 design (not the reference's, which runs one 1024-thread CTA per sweep
+// and a grid.sync() after every step):
+//  * each sweep is owned by one 128-thread CTA; sweeps are pipelined through
+//    point-to-point progress flags (acquire/release, gpu scope) with the
+//    reference's rule (a step at opRow r may run once the previous sweep has
+//    published prog >= r + 2b, :81).  CTAs take sweeps from an atomic ticket,
+//    so any sweep a CTA waits on belongs to a CTA that is already running.
+//  * a step touches band columns [r, r+32) (S2 and B1') and [r-32, r) (B1).
+//    In band storage (ld = 2b) those are contiguous 16 KB tiles: each step
+//    copies one tile (columns [r, r+32), all 64 offsets) into shared memory
+//    with 16-byte cp.async and stores the previous one, instead of gathering
+//    blocks element by element.
+//  * the copy is asynchronous and issued before the Householder vector and the
+//    B1 update, which only need data already in shared memory, so its latency
+//    overlaps that work; the previous tile is stored right after the B1 update.
+//  * S2 <- H S2 H uses the symmetric rank-2 form (y = S u, v = y - (u^T y/2) u,
+//    S -= u v^T + v u^T) and every block update runs on 128 threads (4 per
+//    row/column, two shuffle steps per dot product).
+//  * every wait is bounded in time; on timeout the kernel records an error
+//    word, all CTAs drain, and the host returns EVD_ERR_TIMEOUT.
 #include "common.cuh"
 
 namespace evd {
 
 namespace {
 
-constexpr int kChaseWarpsPerCta = 4;
+constexpr int kBW = 32;                  // band width b
+constexpr int kOff = 2 * kBW;            // band-storage rows per column (2b)
+constexpr int kTileD = kBW * kOff;       // doubles per 32-column tile
+constexpr int kChaseThreads = 128;
 constexpr unsigned long long kWaitTimeoutNs = 4000000000ull;  // 4 s
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -33,179 +46,231 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   return t;
 }
 
-// Lane 0 waits until *flag >= target (or an error is raised elsewhere).
-// Returns false when the sweep must be abandoned.
-__device__ bool warp_wait_geq(const int* flag, int target, int* err, int code) {
-  const int lane = threadIdx.x & 31;
-  int ok = 1;
-  if (lane == 0) {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Thread 0 waits until *flag >= target (or an error is raised elsewhere); the
+// result is broadcast through shared memory.  false = abandon the sweep.
+__device__ bool cta_wait_geq(const int* flag, int target, int* err, volatile int* s_ok) {
+  if (threadIdx.x == 0) {
+    int ok = 1;
     if (ld_acquire(flag) < target) {
       unsigned long long t0 = globaltimer_ns();
       unsigned spins = 0;
       while (ld_acquire(flag) < target) {
-        __nanosleep(40);
-        if ((++spins & 63u) == 0) {
+        __nanosleep(32);
+        if ((++spins & 31u) == 0) {
           if (*(volatile int*)err != 0) {
             ok = 0;
             break;
           }
           if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
-            atomicCAS(err, 0, code);
+            atomicCAS(err, 0, kDevTimeoutChase);
             ok = 0;
             break;
           }
         }
       }
     }
+    *s_ok = ok;
   }
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (ok) (void)ld_acquire(flag);  // every lane acquires
-  return ok != 0;
+  __syncthreads();
+  const bool ok = *s_ok != 0;
+  __syncthreads();  // nobody rewrites s_ok before everyone has read it
+  return ok;
 }
 
-__device__ __forceinline__ void warp_publish(int* flag, int value) {
-  __threadfence();
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) st_release(flag, value);
+// All threads' prior writes -> visible at gpu scope, then thread 0 publishes.
+__device__ __forceinline__ void cta_publish(int* flag, int value) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(flag, value);
+  }
 }
 
-template <int BW>
-__global__ void __launch_bounds__(32 * kChaseWarpsPerCta)
-    chase_kernel(int n, double* __restrict__ sub, long ld, double* __restrict__ U, long ldU,
-                 int* prog, int* ticket, int* err) {
-  constexpr int LD = BW + 1;  // padded row stride of the per-warp tiles
-  constexpr int kPerWarp = 3 * BW * LD + 2 * BW;
-  extern __shared__ double sm[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* base = sm + warp * kPerWarp;
-  double* tB = base;                  // current B1 (row-major, rows = lanes)
-  double* tN = base + BW * LD;        // bulge block B1'
-  double* tS = base + 2 * BW * LD;    // diagonal block S2 (lower part)
-  double* us = base + 3 * BW * LD;    // Householder vector
-  double* vs = us + BW;               // symmetric-update vector
+// Start the copy of band columns [c0, c0+ncol) (all 2b offsets) into smem;
+// columns past ncol are zero-filled.  Completed by cp_async_commit_wait_all().
+__device__ __forceinline__ void tile_load_async(double* t, const double* sub, long c0, int ncol) {
+  const double2* src = reinterpret_cast<const double2*>(sub + c0 * kOff);
+  double2* dst = reinterpret_cast<double2*>(t);
+  const int n2 = ncol * kOff / 2;
+  for (int i = threadIdx.x; i < kTileD / 2; i += kChaseThreads) {
+    if (i < n2) cp_async16(dst + i, src + i);
+    else dst[i] = make_double2(0.0, 0.0);
+  }
+}
+__device__ __forceinline__ void tile_store(double* sub, const double* t, long c0, int ncol) {
+  double2* dst = reinterpret_cast<double2*>(sub + c0 * kOff);
+  const double2* src = reinterpret_cast<const double2*>(t);
+  const int n2 = ncol * kOff / 2;
+  for (int i = threadIdx.x; i < n2; i += kChaseThreads) __stcg(dst + i, src[i]);
+}
+
+struct ChaseSmem {
+  double tile[2][kTileD];  // band columns [base, base+32), element (c, o) at c*64 + o
+  double u[kBW];
+  double v[kBW];
+  double red[4];
+  int ok;
+  int ticket;
+};
+
+__global__ void __launch_bounds__(kChaseThreads)
+    chase_kernel(int n, double* __restrict__ sub, double* __restrict__ U, long ldU, int* prog,
+                 int* ticket, int* err) {
+  __shared__ __align__(16) ChaseSmem sm;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  // 4 threads per row / column: q = index (0..31), p = part (0..3, 8 entries each)
+  const int q = tid >> 2, p = tid & 3;
 
   for (;;) {
-    int s = 0;
-    if (lane == 0) s = atomicAdd(ticket, 1);
-    s = __shfl_sync(0xffffffffu, s, 0);
+    if (tid == 0) {
+      int t = atomicAdd(ticket, 1);
+      if (*(volatile int*)err != 0) t = n;  // drain after an error elsewhere
+      sm.ticket = t;
+    }
+    __syncthreads();
+    const int s = sm.ticket;
+    __syncthreads();
     if (s >= n - 2) break;
-    if (*(volatile int*)err != 0) break;
 
     long r = s + 1;
-    int rb = min(BW, (int)(n - r));
-    int cb = 1;
-    if (s > 0 && !warp_wait_geq(prog + s - 1, (int)(r + 2 * BW), err, kDevTimeoutChase)) break;
-
-    // B1 = column s, rows r .. r+rb-1
-#pragma unroll
-    for (int c = 0; c < BW; ++c) tB[lane * LD + c] = 0.0;
-    if (lane < rb) tB[lane * LD] = __ldcg(sub + (1 + lane) + (long)s * ld);
-    __syncwarp();
+    int rb = min(kBW, (int)(n - r));
+    int cb = 1;  // columns of the previous tile (B1): 1 at the first step
+    int cur = 0;
+    if (s > 0 && !cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) break;
+    // previous tile = column s (its offsets 1..rb hold B1 = A(r:r+rb, s))
+    tile_load_async(sm.tile[1 - cur], sub, s, 1);
+    cp_async_commit_wait_all();
+    __syncthreads();
 
     bool alive = true;
     for (;;) {
-      // Issue every load of this step (diagonal block S2, lower part, and the
-      // bulge block B1' below it) first: one L2 round trip per step, overlapped
-      // with the Householder vector and the B1 update below.
+      double* T = sm.tile[cur];       // columns [r, r+32): S2 and B1'
+      double* P = sm.tile[1 - cur];   // columns [r-cb, r): B1 at offsets cb+i-j
       const long r2 = r + rb;
-      const int rb2 = min(BW, (int)(n - r2));
-      double ls[BW], ln[BW];
-#pragma unroll
-      for (int c = 0; c < BW; ++c)
-        ls[c] = (c <= lane && lane < rb && c < rb) ? __ldcg(sub + (lane - c) + (r + c) * ld) : 0.0;
-#pragma unroll
-      for (int c = 0; c < BW; ++c)
-        ln[c] = (lane < rb2 && c < rb) ? __ldcg(sub + (rb + lane - c) + (r + c) * ld) : 0.0;
+      const int rb2 = min(kBW, (int)(n - r2));
+      // (1) start copying this step's tile; nothing below reads T until (4)
+      tile_load_async(T, sub, r, min(kBW, (int)(n - r)));
 
-      // ---- Householder vector from B1[:,0] (reference convention) ----
-      double x = (lane < rb) ? tB[lane * LD] : 0.0;
-      double nrm2 = warp_sum(x * x);
-      double u = 0.0;
-      if (nrm2 > 0.0) {
-        double scale = 1.0 / sqrt(nrm2);
-        u = x * scale;
-        double u0 = __shfl_sync(0xffffffffu, u, 0);
-        double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
-        if (lane == 0) u = u0n;
-        u *= 1.0 / sqrt(fabs(u0n));
+      // (2) Householder vector from B1[:, 0] = P[0][cb + i]
+      if (warp == 0) {
+        const double x = (lane < rb) ? P[cb + lane] : 0.0;
+        const double nrm2 = warp_sum(x * x);
+        double u = 0.0;
+        if (nrm2 > 0.0) {
+          u = x * (1.0 / sqrt(nrm2));
+          const double u0 = __shfl_sync(0xffffffffu, u, 0);
+          const double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
+          if (lane == 0) u = u0n;
+          u *= 1.0 / sqrt(fabs(u0n));
+        }
+        sm.u[lane] = u;
+        if (lane < rb) U[(r + lane) + (long)s * ldU] = u;
       }
-      us[lane] = u;
-      if (lane < rb) U[(r + lane) + (long)s * ldU] = u;
-      __syncwarp();
+      __syncthreads();
 
-      // ---- B1 <- H B1 (lane c owns column c) ----
-      if (lane < cb) {
-        double v = 0.0;
+      // (3) B1 <- H B1 : column j = q, rows 8p..8p+7 (B1 is rb x cb)
+      {
+        const int j = q;
+        double pv = 0.0;
+        if (j < cb) {
 #pragma unroll
-        for (int l = 0; l < BW; ++l) v = fma(us[l], tB[l * LD + lane], v);
+          for (int k = 0; k < 8; ++k) {
+            const int i = 8 * p + k;
+            pv = fma(sm.u[i], P[j * kOff + cb + i - j], pv);
+          }
+        }
+        pv += __shfl_xor_sync(0xffffffffu, pv, 1);
+        pv += __shfl_xor_sync(0xffffffffu, pv, 2);
+        if (j < cb) {
 #pragma unroll
-        for (int l = 0; l < BW; ++l) tB[l * LD + lane] = fma(-v, us[l], tB[l * LD + lane]);
-      }
-      __syncwarp();
-      // write back B1: element (r+l, r-cb+c) -> sub[(cb+l-c) + (r-cb+c)*ld]
-      for (int c = 0; c < cb; ++c)
-        if (lane < rb) __stcg(sub + (cb + lane - c) + (r - cb + c) * ld, tB[lane * LD + c]);
-
-      // ---- S2 <- H S2 H  (symmetric rank-2 form, lower part stored) ----
-#pragma unroll
-      for (int c = 0; c < BW; ++c) tS[lane * LD + c] = ls[c];
-#pragma unroll
-      for (int c = 0; c < BW; ++c) tN[lane * LD + c] = ln[c];
-      __syncwarp();
-      double y = 0.0;
-      if (lane < rb) {
-#pragma unroll
-        for (int c = 0; c < BW; ++c) {
-          if (c < rb) {
-            double sv = (c <= lane) ? tS[lane * LD + c] : tS[c * LD + lane];
-            y = fma(sv, us[c], y);
+          for (int k = 0; k < 8; ++k) {
+            const int i = 8 * p + k;
+            if (i < rb) P[j * kOff + cb + i - j] = fma(-pv, sm.u[i], P[j * kOff + cb + i - j]);
           }
         }
       }
-      double tt = warp_sum(u * y);
-      double v = y - 0.5 * tt * u;
-      vs[lane] = v;
-      __syncwarp();
-      if (lane < rb) {
-#pragma unroll
-        for (int c = 0; c < BW; ++c)
-          if (c <= lane) tS[lane * LD + c] -= u * vs[c] + v * us[c];
-      }
-      __syncwarp();
-      for (int c = 0; c < rb; ++c)
-        if (lane >= c && lane < rb) __stcg(sub + (lane - c) + (r + c) * ld, tS[lane * LD + c]);
+      __syncthreads();
+      // the previous tile (S2 of the last step + this B1) is now final
+      tile_store(sub, P, r - cb, cb);
+      // (4) this thread's copies of T are done; the barrier makes all visible
+      cp_async_commit_wait_all();
+      __syncthreads();
 
-      // ---- bulge block B1' (rows r2.., cols r..r+rb-1) <- B1' H ----
+      // (5) S2 <- H S2 H  with S(i, j) = T[j][i-j] (i >= j)
+      {
+        const int i = q;
+        double y = 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int j = 8 * p + k;
+          const double sv = (j <= i) ? T[j * kOff + (i - j)] : T[i * kOff + (j - i)];
+          y = fma(sv, sm.u[j], y);
+        }
+        y += __shfl_xor_sync(0xffffffffu, y, 1);
+        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        // t = u^T y over the 32 rows: rows 8w..8w+7 live in warp w (p == 0 lanes)
+        double uy = (p == 0) ? sm.u[i] * y : 0.0;
+        uy = warp_sum(uy);
+        if (lane == 0) sm.red[warp] = uy;
+        __syncthreads();
+        const double t = (sm.red[0] + sm.red[1]) + (sm.red[2] + sm.red[3]);
+        const double vi = y - 0.5 * t * sm.u[i];
+        if (p == 0) sm.v[i] = vi;
+        __syncthreads();
+        const double ui = sm.u[i];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int j = 8 * p + k;
+          if (j <= i && i < rb) T[j * kOff + (i - j)] -= ui * sm.v[j] + vi * sm.u[j];
+        }
+      }
+      // (6) B1' <- B1' H : row i = q (rows r+rb+i), N(i, j) = T[j][rb + i - j].
+      // S2 owns offsets <= rb-1-j of column j, B1' offsets >= rb-j: no overlap.
       if (rb2 > 0) {
+        const int i = q;
         double w = 0.0;
 #pragma unroll
-        for (int c = 0; c < BW; ++c) w = fma(tN[lane * LD + c], us[c], w);
+        for (int k = 0; k < 8; ++k) {
+          const int j = 8 * p + k;
+          if (j < rb) w = fma(T[j * kOff + rb + i - j], sm.u[j], w);
+        }
+        w += __shfl_xor_sync(0xffffffffu, w, 1);
+        w += __shfl_xor_sync(0xffffffffu, w, 2);
+        if (i < rb2) {
 #pragma unroll
-        for (int c = 0; c < BW; ++c) tN[lane * LD + c] = fma(-w, us[c], tN[lane * LD + c]);
+          for (int k = 0; k < 8; ++k) {
+            const int j = 8 * p + k;
+            if (j < rb) T[j * kOff + rb + i - j] = fma(-w, sm.u[j], T[j * kOff + rb + i - j]);
+          }
+        }
       }
-      __syncwarp();
       if (rb2 <= 1) {
-        if (rb2 == 1 && lane < rb) __stcg(sub + (rb - lane) + (r + lane) * ld, tN[lane]);
-        warp_publish(prog + s, n + 3 * BW);
+        __syncthreads();
+        tile_store(sub, T, r, min(kBW, (int)(n - r)));
+        cta_publish(prog + s, n + 3 * kBW);
         break;
       }
-      warp_publish(prog + s, (int)r2);
-
+      cta_publish(prog + s, (int)r2);
       cb = rb;
       rb = rb2;
       r = r2;
-      double* tmp = tB;
-      tB = tN;
-      tN = tmp;
-      if (s > 0 && !warp_wait_geq(prog + s - 1, (int)(r + 2 * BW), err, kDevTimeoutChase)) {
+      cur = 1 - cur;
+      if (s > 0 && !cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) {
         alive = false;
         break;
       }
     }
     if (!alive) break;
-    // restore tile roles for the next sweep
-    tB = base;
-    tN = base + BW * LD;
+    __syncthreads();
   }
 }
 
@@ -236,7 +301,7 @@ int band_pack(long n, long b, const double* dA, long ldA, double* dSub, long ldS
   if (n == 0) return EVD_SUCCESS;
   dim3 blk(32, 8);
   band_pack_kernel<<<ceil_div_i(n, 8), blk, 0, st>>>((int)n, (int)b, dA, ldA, dSub, ldSub);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
@@ -244,9 +309,12 @@ long chase_iwork_ints(long n) { return n + 64; }
 
 // Launch the chase; does not synchronise.  iwork: chase_iwork_ints(n) ints.
 // The error word is iwork[n + 32] (0 = ok).
+// The tile copies need ldSub == 2b exactly (contiguous band columns) and a
+// 16-byte aligned dSub.
 int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
                       double* d, double* e, int* iwork, cudaStream_t st) {
-  if (n < 0 || b != 32 || ldSub < 2 * b || (n > 0 && ldU < n)) return EVD_ERR_INVALID_ARG;
+  if (n < 0 || b != kBW || ldSub != 2 * b || (n > 0 && ldU < n)) return EVD_ERR_INVALID_ARG;
+  if (((uintptr_t)dSub & 15u) != 0) return EVD_ERR_INVALID_ARG;
   if (n > (1L << 30)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (!dSub || !d || !iwork || (n > 2 && !dU) || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;
@@ -255,24 +323,16 @@ int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long
   int* err = iwork + n + 32;
   EVD_CUDA_TRY(cudaMemsetAsync(iwork, 0, sizeof(int) * chase_iwork_ints(n), st));
   if (n > 2) {
-    constexpr int BW = 32;
-    constexpr size_t smem = kChaseWarpsPerCta * (3 * BW * (BW + 1) + 2 * BW) * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
-      EVD_CUDA_TRY(cudaFuncSetAttribute(chase_kernel<BW>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      attr = true;
-    }
-    long sweeps = n - 2;
-    long max_workers = 2L * device_sm_count() * kChaseWarpsPerCta;
-    long workers = std::min(sweeps, max_workers);
-    int ctas = ceil_div_i(workers, kChaseWarpsPerCta);
-    chase_kernel<BW><<<ctas, 32 * kChaseWarpsPerCta, smem, st>>>((int)n, dSub, ldSub, dU, ldU,
-                                                                 prog, ticket, err);
-    EVD_CUDA_TRY(cudaGetLastError());
+    // enough CTAs for the pipeline's concurrency (a sweep starts every 3 steps
+    // and lasts about n/b steps), bounded by the GPU's resident capacity
+    const long sweeps = n - 2;
+    const long want = n / (3 * kBW) + 16;
+    const int ctas = (int)std::min(std::min(sweeps, want), 6L * device_sm_count());
+    chase_kernel<<<ctas, kChaseThreads, 0, st>>>((int)n, dSub, dU, ldU, prog, ticket, err);
+    EVD_LAUNCHED();
   }
   band_to_tridiag_kernel<<<ceil_div_i(n, 256), 256, 0, st>>>((int)n, dSub, ldSub, d, e);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 

@@ -25,6 +25,14 @@
     }                                                                             \
   } while (0)
 
+// Every kernel launch site ends with EVD_LAUNCHED(): counts the launch (see
+// evd_launch_count) and surfaces launch errors.
+#define EVD_LAUNCHED()                          \
+  do {                                          \
+    ::evd::note_launch();                       \
+    EVD_CUDA_TRY(cudaGetLastError());           \
+  } while (0)
+
 #define EVD_TRY(call)                          \
   do {                                         \
     int evd_st__ = (call);                     \
@@ -71,6 +79,7 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 inline int ceil_div_i(long a, long b) { return (int)((a + b - 1) / b); }
 
 int device_sm_count();
+void note_launch();
 
 // Reads a device error word written by a kernel (synchronises `st`) and maps
 // it to an EVD_* status.

@@ -308,7 +308,7 @@ int launch_cfg(GemmArgs p, int grid_x, int grid_y, cudaStream_t st) {
     attr_set = true;
   }
   kern<<<dim3(grid_x, grid_y), NT, smem, st>>>(p);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
@@ -377,7 +377,7 @@ static int gemm_run(GemmArgs p, bool ta, bool tb, long batch, cudaStream_t st,
     int blocks = (int)std::min<long>((total + 255) / 256, 4L * device_sm_count());
     dgemm_splitk_reduce_kernel<<<blocks, 256, 0, st>>>(p.m, p.n, p.splitk, batch, p.ws,
                                                        p.alpha, p.beta, p.C, p.ldc, p.sC);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
   }
   return EVD_SUCCESS;
 }

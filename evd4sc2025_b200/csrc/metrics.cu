@@ -57,16 +57,34 @@ __global__ void final_sum_kernel(int nparts, const double* __restrict__ partial,
   }
 }
 
+// Reduction partials of the metrics (8 KB, module scope): the reference gives
+// checkOrthogonality exactly an M x M work buffer, so the partial sums cannot
+// live there.  Calls that overlap on the GPU share it.
+__device__ double g_metric_partials[kRedBlocks + 16];
+
 }  // namespace
+
+static int metric_scratch(double** p) {
+  static double* dev = nullptr;  // per process; the runtime keeps one module per device
+  int d = -1;
+  static int dev_id = -2;
+  EVD_CUDA_TRY(cudaGetDevice(&d));
+  if (dev == nullptr || d != dev_id) {
+    EVD_CUDA_TRY(cudaGetSymbolAddress((void**)&dev, g_metric_partials));
+    dev_id = d;
+  }
+  *p = dev;
+  return EVD_SUCCESS;
+}
 
 // sqrt(sum (M - shift I - Y diag(w))^2) into *dout (device); scratch >= kRedBlocks doubles
 int frob_norm_dev(long m, long n, const double* M, long ldm, double shift, const double* Y,
                   long ldy, const double* w, double* scratch, double* dout, cudaStream_t st) {
   int blocks = (int)std::min<long>(kRedBlocks, std::max<long>(1, (m * n + 255) / 256));
   sumsq_kernel<<<blocks, kRedThreads, 0, st>>>(m, n, M, ldm, shift, Y, ldy, w, scratch);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   final_sum_kernel<<<1, 256, 0, st>>>(blocks, scratch, dout);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
@@ -80,7 +98,8 @@ extern "C" int evd_check_orthogonality(long M, long N, const double* dA, long ld
   // The reference computes A^T B with A, B of M columns and N rows
   // (cublasDgemm(T, N, M, M, N, ...)); work holds the M x M product.
   EVD_TRY(evd::dgemm('t', 'n', M, M, N, 1.0, dA, ldA, dB, ldB, 0.0, work, M, stream));
-  double* scratch = work + M * M;
+  double* scratch = nullptr;
+  EVD_TRY(evd::metric_scratch(&scratch));
   EVD_TRY(evd::frob_norm_dev(M, M, work, M, 1.0, nullptr, 0, nullptr, scratch + 8, scratch,
                              stream));
   double h = 0.0;
@@ -94,9 +113,10 @@ extern "C" int evd_check_eig(long n, const double* A, long lda, const double* w,
                              long ldX, double* work, double* result, cudaStream_t stream) {
   if (n <= 0 || lda < n || ldX < n || !A || !w || !X || !work || !result)
     return EVD_ERR_INVALID_ARG;
-  double* AX = work;               // n x n
-  double* scratch = work + n * n;  // reduction scratch (needs ~600 doubles; work >= 2 n^2)
-  double* sums = scratch;          // [0] resid^2 [1] ||A||^2 [2] orth^2
+  double* AX = work;  // n x n
+  double* scratch = nullptr;
+  EVD_TRY(evd::metric_scratch(&scratch));
+  double* sums = scratch;    // [0] resid^2 [1] ||A||^2 [2] orth^2
   double* part = scratch + 8;
   EVD_TRY(evd::dgemm('n', 'n', n, n, n, 1.0, A, lda, X, ldX, 0.0, AX, n, stream));
   EVD_TRY(evd::frob_norm_dev(n, n, AX, n, 0.0, X, ldX, w, part, sums + 0, stream));

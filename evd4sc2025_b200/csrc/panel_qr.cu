@@ -53,23 +53,29 @@ TsqrPlan make_plan(long m) {
   int L = 0;
   p.rows[0] = (int)m;
   p.T[0] = ceil_div_i(m, kTile);
-  long off = 0;
   int coff = 0;
   while (p.T[L] > 1 && L + 1 < kMaxLevels) {
     p.rows[L + 1] = kNB * p.T[L];
     p.T[L + 1] = ceil_div_i(p.rows[L + 1], kTile);
-    p.soff[L + 1] = off;
-    off += (long)p.rows[L + 1] * kNB;
     p.coff[L + 1] = coff;
     coff += p.T[L + 1];
     ++L;
   }
   p.nlev = L + 1;
+  p.ncnt = coff;
+  // Arrival counters come first, at a fixed offset: a workspace sized (and
+  // zeroed) for the largest panel then serves every smaller panel, whose
+  // counters are a prefix of the same region (the kernels reset each counter
+  // after use).
+  p.cnt_off = 0;
+  long off = (coff + 1) / 2 + 2;  // ints packed two per double
+  off = (off + 1) / 2 * 2;        // keep the stacks 16-byte aligned
+  for (int l = 1; l < p.nlev; ++l) {
+    p.soff[l] = off;
+    off += (long)p.rows[l] * kNB;
+  }
   p.qtop_off = off;
   off += kNB * kNB;
-  p.cnt_off = off;
-  p.ncnt = coff;
-  off += (coff + 1) / 2 + 2;  // ints packed two per double
   p.total = off;
   return p;
 }
@@ -456,11 +462,11 @@ int panel_qr_launch(long m, double* A, long lda, double* ws, int mode, double* Y
   TsqrPlan plan = make_plan(m);
   if (plan.nlev >= kMaxLevels) return EVD_ERR_INVALID_ARG;
   tsqr_up_kernel<<<plan.T[0], kThreads, 0, st>>>(plan, A, lda, ws, R, ldr);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   EVD_TRY(finish_attr());
   tsqr_finish_kernel<<<plan.T[0], kThreads, kFinishDyn, st>>>(plan, ws, A, lda, mode, Yout, ldy,
                                                               Wout, ldw, R, ldr, Aband, ldband);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 

@@ -8,7 +8,8 @@ namespace evd {
 // arrival counters).
 long panel_qr_ws_doubles(long m);
 int panel_qr_check(long m, long n, long lda);
-// Zero the arrival counters (needed once per workspace; the kernels reset them).
+// Zero the arrival counters for panels of up to m rows (needed once per
+// workspace; the kernels reset each counter after use).
 int panel_counters_reset(long m, double* ws, cudaStream_t st);
 // mode 0: A <- explicit thin Q.  mode 1: Yout <- Y, Wout <- W, R <- R and, if
 // Aband != nullptr, the panel of the band matrix (R over zeros) into Aband.

@@ -33,7 +33,7 @@ int set_identity(long m, long n, double* Q, long ldq, cudaStream_t st) {
   if (m <= 0 || n <= 0) return EVD_SUCCESS;
   dim3 grid(ceil_div_i(m, 256), (unsigned)std::min<long>(n, 65535));
   set_identity_kernel<<<grid, 256, 0, st>>>(m, n, Q, ldq);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 

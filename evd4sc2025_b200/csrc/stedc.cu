@@ -107,15 +107,26 @@ __global__ void absmax_kernel(long n, const double* d, const double* e, double* 
   __shared__ double red[32];
   double m = 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    m = fmax(m, fabs(d[i]));
-    if (i < n - 1) m = fmax(m, fabs(e[i]));
+    const double a = fabs(d[i]), b = (i < n - 1) ? fabs(e[i]) : 0.0;
+    // fmax drops NaN; keep it visible so the host can reject the input
+    m = (isnan(a) || isnan(b)) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(m, fmax(a, b));
+    if (isnan(m)) break;
   }
-  m = warp_max(m);
+  // NaN-propagating max over the block
+#pragma unroll
+  for (int k = 16; k > 0; k >>= 1) {
+    double o = __shfl_xor_sync(0xffffffffu, m, k);
+    m = (isnan(o) || isnan(m)) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(m, o);
+  }
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x < 32) {
     double t = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0.0;
-    t = warp_max(t);
+#pragma unroll
+    for (int k = 16; k > 0; k >>= 1) {
+      double o = __shfl_xor_sync(0xffffffffu, t, k);
+      t = (isnan(o) || isnan(t)) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(t, o);
+    }
     if (threadIdx.x == 0) out[0] = t;
   }
 }
@@ -242,6 +253,7 @@ struct LevelArgs {
   double* Zw;
   double *zv, *ds, *zs, *dK, *zK, *tau, *zh, *dD, *rc, *rs, *rho;
   int *perm, *colK, *typK, *pT, *pB, *colD, *rA, *rB, *org, *desc;
+  int* err;
   double *Qt, *Qb, *Ut, *Ub, *Zn;
   int K12max, K23max, Kmax;
 };
@@ -316,6 +328,10 @@ __global__ void merge_deflate_kernel(LevelArgs a) {
     for (int k = 0; k < N; ++k) {
       double dk = ds[k], zk = zs[k];
       int ck = perm[k];
+      if (ck < 0 || ck >= N) {
+        atomicCAS(a.err, 0, kDevBadShape);
+        return;
+      }
       int tk = (ck < n1) ? 1 : 3;
       if (rho * fabs(zk) <= tol) {
         a.dD[lo + nd] = dk;
@@ -397,6 +413,10 @@ __global__ void merge_rotate_kernel(LevelArgs a) {
   double* row = a.Zw + (lo + r) + lo * a.ldz;
   for (int q = 0; q < nr; ++q) {
     long ca = a.rA[lo + q], cb = a.rB[lo + q];
+    if (ca < 0 || ca >= a.N || cb < 0 || cb >= a.N) {
+      atomicCAS(a.err, 0, kDevBadShape);
+      return;
+    }
     double c = a.rc[lo + q], s = a.rs[lo + q];
     double x = row[ca * a.ldz], y = row[cb * a.ldz];
     row[ca * a.ldz] = c * x + s * y;
@@ -424,6 +444,10 @@ __global__ void merge_gather_kernel(LevelArgs a) {
   }
   for (int i = 0; i < K; ++i) {
     long col = a.colK[lo + i];
+    if (col < 0 || col >= a.N) {
+      atomicCAS(a.err, 0, kDevBadShape);
+      return;
+    }
     double v = zrow[col * a.ldz];
     if (r < a.n1) {
       int p = a.pT[lo + i];
@@ -446,8 +470,16 @@ __global__ void merge_copy_deflated_kernel(LevelArgs a) {
   const int K = d_[D_K], nd = d_[D_NDEF];
   const double* zrow = a.Zw + (lo + r) + lo * a.ldz;
   double* Zn = a.Zn + (long)m * a.N * a.N;
+  if (K + nd > a.N) {
+    atomicCAS(a.err, 0, kDevBadShape);
+    return;
+  }
   for (int t = 0; t < nd; ++t) {
     long col = a.colD[lo + t];
+    if (col < 0 || col >= a.N) {
+      atomicCAS(a.err, 0, kDevBadShape);
+      return;
+    }
     Zn[r + (long)(K + t) * a.N] = zrow[col * a.ldz];
   }
 }
@@ -666,6 +698,10 @@ __global__ void merge_scatter_kernel(LevelArgs a) {
   const double* Zn = a.Zn + (long)m * a.N * a.N;
   for (int p = 0; p < a.N; ++p) {
     int q = a.perm[lo + p];
+    if (q < 0 || q >= a.N) {
+      atomicCAS(a.err, 0, kDevBadShape);
+      return;
+    }
     a.Zw[(lo + r) + (lo + p) * a.ldz] = Zn[r + (long)q * a.N];
   }
   if (r == 0)
@@ -708,17 +744,25 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
   int* err = iwork + P.i_desc + 8 * (np / 2 + 1) + 8;
   EVD_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), st));
   absmax_kernel<<<1, 1024, 0, st>>>(n, d, e, scal);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
+  {
+    // A NaN or Inf entry would break the merge ordering (ranks of NaN keys
+    // collide); reject it before any merge runs.
+    double h = 0.0;
+    EVD_CUDA_TRY(cudaMemcpyAsync(&h, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EVD_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!isfinite(h)) return EVD_ERR_INVALID_ARG;
+  }
   double* dw = work + P.o_d;
   double* ew = work + P.o_e;
   double* Zw = work + P.o_Z;
   init_kernel<<<ceil_div_i(np, 256), 256, 0, st>>>(n, np, P.s, d, e, scal, dw, ew);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   EVD_CUDA_TRY(cudaMemsetAsync(Zw, 0, sizeof(double) * np * np, st));
   const int nleaves = 1 << P.L;
   leaf_ql_kernel<<<ceil_div_i((long)nleaves * 32, 128), 128, 0, st>>>(P.s, nleaves, dw, ew, Zw,
                                                                        np, err);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
 
   std::vector<int> hdesc;
   for (int lev = 1; lev <= P.L; ++lev) {
@@ -753,6 +797,7 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     a.rB = iwork + P.i_rB;
     a.org = iwork + P.i_org;
     a.desc = iwork + P.i_desc;
+    a.err = err;
     a.Qt = work + P.o_Qt;
     a.Qb = work + P.o_Qb;
     a.Ut = work + P.o_Ut;
@@ -760,9 +805,9 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     a.Zn = work + P.o_Zn;
     dim3 gN(ceil_div_i(a.N, 256), a.nm);
     merge_setup_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
     merge_deflate_kernel<<<a.nm, 32, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
     hdesc.resize(8 * a.nm);
     EVD_CUDA_TRY(cudaMemcpyAsync(hdesc.data(), a.desc, sizeof(int) * 8 * a.nm,
                                  cudaMemcpyDeviceToHost, st));
@@ -780,18 +825,18 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     a.K23max = K23;
     if (nrmax > 0) {
       merge_rotate_kernel<<<gN, 256, 0, st>>>(a);
-      EVD_CUDA_TRY(cudaGetLastError());
+      EVD_LAUNCHED();
     }
     merge_gather_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
     if (Kmax > 0) {
       dim3 gK(ceil_div_i(Kmax, 128), a.nm);
       merge_secular_kernel<<<gK, 128, 0, st>>>(a);
-      EVD_CUDA_TRY(cudaGetLastError());
+      EVD_LAUNCHED();
       merge_loewner_kernel<<<gK, 128, 0, st>>>(a);
-      EVD_CUDA_TRY(cudaGetLastError());
+      EVD_LAUNCHED();
       merge_vectors_kernel<<<dim3(Kmax, a.nm), 256, 0, st>>>(a);
-      EVD_CUDA_TRY(cudaGetLastError());
+      EVD_LAUNCHED();
       // Zn[0:n1, 0:Kmax] = Qt Ut ; Zn[n1:N, 0:Kmax] = Qb Ub   (batched over merges)
       const long sZ = (long)a.N * a.N;
       if (K12 > 0) {
@@ -813,15 +858,15 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
       }
     }
     merge_copy_deflated_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
     merge_finalize_rank_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
     merge_scatter_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_CUDA_TRY(cudaGetLastError());
+    EVD_LAUNCHED();
   }
   dim3 gf(ceil_div_i(n, 256), (unsigned)std::min<long>(n, 65535));
   finish_kernel<<<gf, 256, 0, st>>>(n, np, dw, Zw, np, scal, d, Z, ldz);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return read_device_error(err, st);
 }
 

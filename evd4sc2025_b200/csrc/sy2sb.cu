@@ -104,7 +104,7 @@ int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, lo
       dim3 grid(ceil_div_i(Nf, 256), (unsigned)std::min<long>(nb, 65535));
       copy_block_kernel<<<grid, 256, 0, st>>>(Nf, nb, OA + off + off * ldOA, ldOA,
                                               dA + off + off * ldA, ldA);
-      EVD_CUDA_TRY(cudaGetLastError());
+      EVD_LAUNCHED();
     }
     for (long i = b; i <= nb && i < Nf; i += b) {
       const long m = Nf - i;
@@ -150,7 +150,7 @@ int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, lo
   // dA <- symmetric band (copyMatrixL2U, src/EVD/myEVD.cu:346)
   dim3 g2(ceil_div_i(M, 32), ceil_div_i(M, 32));
   mirror_l2u_kernel<<<g2, dim3(32, 8), 0, st>>>(M, dA, ldA);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
@@ -158,7 +158,7 @@ int mirror_l2u(long n, double* A, long lda, cudaStream_t st) {
   if (n <= 0) return EVD_SUCCESS;
   dim3 g2(ceil_div_i(n, 32), ceil_div_i(n, 32));
   mirror_l2u_kernel<<<g2, dim3(32, 8), 0, st>>>(n, A, lda);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
@@ -167,7 +167,7 @@ int copy_matrix(long m, long n, const double* src, long lds, double* dst, long l
   if (m <= 0 || n <= 0) return EVD_SUCCESS;
   dim3 grid(ceil_div_i(m, 256), (unsigned)std::min<long>(n, 65535));
   copy_block_kernel<<<grid, 256, 0, st>>>(m, n, src, lds, dst, ldd);
-  EVD_CUDA_TRY(cudaGetLastError());
+  EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 

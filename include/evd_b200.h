@@ -36,6 +36,15 @@ const char* evd_status_string(int status);
 /* Library version string, e.g. "evd_b200 0.1 sm_100a". */
 const char* evd_version(void);
 
+/* Number of kernel launches this library has issued since it was loaded (host
+ * counter; a measurement aid with no counterpart in the reference). */
+long evd_launch_count(void);
+
+/* Measured FP64 DMMA throughput of the current GPU in TFLOP/s (a short
+ * microbenchmark; the roofline denominator for the FP64 kernels; no
+ * counterpart in the reference).  Synchronises `stream`. */
+int evd_fp64_peak_probe(double* tflops, cudaStream_t stream);
+
 /* ---- FP64 GEMM / SYR2K building blocks --------------------------------- */
 
 /* C = alpha*op(A)*op(B) + beta*C, op = N ('n') or T ('t'); FP64 on DMMA.
@@ -110,7 +119,8 @@ int evd_band_pack(long n, long b, const double* dA, long ldA, double* dSub, long
 /* Bytes of int scratch needed by evd_bulge_chase (progress flags + counters). */
 long evd_bulge_chase_iwork_size(long n);
 
-/* Band -> tridiagonal.  dSub is band storage (ldSub >= 2b) and is overwritten;
+/* Band -> tridiagonal.  dSub is band storage with ldSub == 2b exactly (each
+ * column contiguous) and 16-byte alignment; it is overwritten;
  * every Householder vector (||u||^2 = 2) is written into dU column s (sweep s),
  * 32-row segments starting at row s+1, exactly where chasing_kernel_one_timeV10
  * writes them (util/inc/bugle_chasingV10.h:21-392, launched at
@@ -152,8 +162,8 @@ int evd_bc_back_apply(long n, long ncols, const double* U, long ldU, double* X, 
 /* Merge the b-wide compact-WY slides of an M x N block into one compact WY:
  * W[:, i-b:i] -= W[:, 0:i-b] * (Y[:, 0:i-b]^T * W[:, i-b:i]) for i = 2b..N.
  * Same as computerWYFromSlide (api/inc/computerWYFromSlide.h:4,
- * api/computerWYFromSlide.cu:5-25); work >= M*N doubles is unused here but kept
- * for signature parity (pass NULL to skip). */
+ * api/computerWYFromSlide.cu:5-25); work >= M*b doubles (the reference's
+ * (i-b) x b product with leading dimension M). */
 int evd_wy_from_slide(long M, long N, long slideWidth, double* dW, long ldW,
                       const double* dY, long ldY, double* work, cudaStream_t stream);
 
@@ -179,12 +189,13 @@ int evd_sbr_back(long n, long b, long nk, double* dW, long ldW, const double* dY
 
 /* result[0] = ||A^T B - I||_F / M  (checkOrthogonality,
  * util/tool/checkMetric.cu:5-24, which prints instead of returning).
- * work >= M*M doubles. */
+ * A and B are N x M.  work >= M*M doubles (as the reference); result is a
+ * HOST pointer (the call synchronises `stream`). */
 int evd_check_orthogonality(long M, long N, const double* dA, long ldA, const double* dB,
                             long ldB, double* work, double* result, cudaStream_t stream);
 
 /* result[0] = ||A X - X diag(w)||_F / (n ||A||_F), result[1] = ||X^T X - I||_F / n.
- * work >= 2*n*n doubles. */
+ * work >= n*n doubles; result is a HOST pointer (synchronises `stream`). */
 int evd_check_eig(long n, const double* A, long lda, const double* w, const double* X,
                   long ldX, double* work, double* result, cudaStream_t stream);
 
