@@ -16,16 +16,18 @@
 // that: the overlap of strip R's sweep h with strip R+-256 occurs only for
 // sweeps on the correct side.  (The reference uses the forward order.)
 //
-// B200 layout (not the reference's): a warp owns 4 columns of X and holds the
+// B200 layout (not the reference's): a warp owns 8 columns of X and holds the
 // 256-row window in registers, lane l holding rows 8l..8l+7 of each column,
-// so a 32-row reflector is 4 lanes (2 shuffle steps per dot product) and each
-// reflector value read from shared memory feeds 4 columns.  The window slides
-// one row per sweep through a ring of 8 registers (the phase is a
-// compile-time constant inside an 8-sweep block), so the slide costs one
-// shuffle per column and no register moves; the row leaving the window is
-// written back and the row entering is prefetched one block ahead.  Reflector
-// chunks (32 sweeps x 256 rows) are double-buffered in shared memory with
-// cp.async.  Exactly 2 n^2 ncols flops, FP64 FMA; rows >= n are never read or
+// so a 32-row reflector is 4 lanes (2 shuffle steps per dot product, eight
+// independent dot products per sweep) and each reflector value read from
+// shared memory feeds 8 columns.  The window slides one row per sweep through
+// a ring of 8 registers (the phase is a compile-time constant inside an
+// 8-sweep block): one rotation shuffle per column, no register moves, no
+// divergent branches; the row leaving the window is written back and the row
+// entering is prefetched one block ahead.  Reflector chunks (16 sweeps x 256
+// rows) are double-buffered in shared memory with cp.async, in a rotated
+// layout that is bank-conflict free for both the copy and the reads; 4-warp
+// CTAs so that two or more fit per SM.  Exactly 2 n^2 ncols flops, FP64 FMA; rows >= n are never read or
 // written (the reference needs 346 zero rows of padding).
 #include "common.cuh"
 
@@ -34,9 +36,9 @@ namespace evd {
 namespace {
 
 constexpr int kWin = 256;   // window rows (8 reflectors of 32)
-constexpr int kCols = 4;    // columns per warp
-constexpr int kWarps = 8;   // warps per CTA
-constexpr int kChunk = 32;  // sweeps per staged reflector chunk
+constexpr int kCols = 8;    // columns per warp
+constexpr int kWarps = 4;   // warps per CTA
+constexpr int kChunk = 16;  // sweeps per staged reflector chunk
 constexpr int kThreadsBC = kWarps * 32;
 
 __device__ __forceinline__ void cp_async8_zfill(double* smem, const double* gmem, bool valid) {
@@ -48,38 +50,44 @@ __device__ __forceinline__ void cp_async8_zfill(double* smem, const double* gmem
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Stage reflectors of sweeps [h0, h0+kChunk) for strip R into buf, layout
-// buf[hc*256 + j*32 + l] = U(R+h+1 + 8l+j, h) (zero for h >= H or row >= n).
+// Shared-memory slot of window row i = 8l + j of one staged sweep: lane l reads
+// its 8 values at j*32 + rot(l, j); the rotation by 4j keeps both the staging
+// writes (consecutive rows) and the per-sweep reads (consecutive lanes) free
+// of bank conflicts.
+__device__ __forceinline__ int uslot(int l, int j) { return j * 32 + ((l + 4 * j) & 31); }
+
+// Stage reflectors of sweeps [h0, h0+kChunk) for strip R (zero for h >= H or
+// row >= n): buf[hc*256 + uslot(l, j)] = U(R+h+1 + 8l+j, h).
 __device__ __forceinline__ void stage_chunk(double* buf, const double* U, long ldU, int n, long R,
                                             int H, int h0) {
   for (int e = threadIdx.x; e < kChunk * kWin; e += kThreadsBC) {
-    int hc = e >> 8, i = e & 255;       // i = window row
+    int hc = e >> 8, i = e & 255;
     int h = h0 + hc;
     long row = R + h + 1 + i;
     bool valid = (h < H) && (row < n);
     const double* src = valid ? (U + row + (long)h * ldU) : U;
-    int l = i >> 3, j = i & 7;
-    cp_async8_zfill(buf + hc * kWin + j * 32 + l, src, valid);
+    cp_async8_zfill(buf + hc * kWin + uslot(i >> 3, i & 7), src, valid);
   }
 }
 
 template <bool FWD>
-__global__ void __launch_bounds__(kThreadsBC, 1)
+__global__ void __launch_bounds__(kThreadsBC, 2)
     q2_apply_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
                     double* __restrict__ X, long ldX) {
   extern __shared__ double smem[];
   double* Ubuf = smem;                                   // 2 x kChunk x kWin
-  double* iobase = smem + 2 * kChunk * kWin;             // per warp: in[2][8][4], out[8][4]
+  double* iobase = smem + 2 * kChunk * kWin;             // per warp: in[2][8][C], out[8][C]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* inbuf = iobase + warp * (3 * 8 * kCols);
   double* outbuf = inbuf + 2 * 8 * kCols;
   const int col0 = blockIdx.x * (kWarps * kCols) + warp * kCols;
 
-  // per-lane I/O column (row r = lane/4, column c = lane%4) for block transfers
+  // block transfers of 8 rows x 8 columns: lane -> (row r = lane/4, columns c0, c0+4)
   const int io_r = lane >> 2, io_c = lane & 3;
-  const int io_col = col0 + io_c;
-  const bool io_col_ok = io_col < ncols;
-  double* io_colp = X + (long)(io_col_ok ? io_col : 0) * ldX;
+  const int io_colA = col0 + io_c, io_colB = col0 + io_c + 4;
+  const bool okA = io_colA < ncols, okB = io_colB < ncols;
+  double* colA = X + (long)(okA ? io_colA : 0) * ldX;
+  double* colB = X + (long)(okB ? io_colB : 0) * ldX;
 
   const int nstrips = (n - 2 + kWin - 1) / kWin;
   for (int si = 0; si < nstrips; ++si) {
@@ -103,105 +111,100 @@ __global__ void __launch_bounds__(kThreadsBC, 1)
         x[c][j] = (col < ncols && row < n) ? X[row + (long)col * ldX] : 0.0;
       }
     }
-    // first reflector chunk + first incoming block
     __syncthreads();
-    {
-      int hc0 = FWD ? 0 : (nchunks - 1) * kChunk;
-      stage_chunk(Ubuf, U, ldU, n, R, H, hc0);
-      cp_commit();
-    }
-    // incoming rows for block 0: FWD rows ws(h)+256 for h = 0..7 -> R+257+r;
-    // REV rows ws(h)-1 = R+h for h = Hp-1 .. Hp-8 -> R+Hp-1-r
+    stage_chunk(Ubuf, U, ldU, n, R, H, FWD ? 0 : (nchunks - 1) * kChunk);
+    cp_commit();
+    // incoming rows for block 0: FWD rows R+257+r; REV rows R+Hp-1-r
     {
       long row = FWD ? (R + 257 + io_r) : (R + Hp - 1 - io_r);
-      inbuf[io_r * kCols + io_c] = (io_col_ok && row < n && row >= 0) ? io_colp[row] : 0.0;
+      const bool rok = row < n && row >= 0;
+      inbuf[io_r * kCols + io_c] = (okA && rok) ? colA[row] : 0.0;
+      inbuf[io_r * kCols + io_c + 4] = (okB && rok) ? colB[row] : 0.0;
     }
 
     for (int ck = 0; ck < nchunks; ++ck) {
       const int chunk = FWD ? ck : (nchunks - 1 - ck);
-      double* cur = Ubuf + (ck & 1) * (kChunk * kWin);
+      const double* cur = Ubuf + (ck & 1) * (kChunk * kWin);
       cp_wait_all();
       __syncthreads();
-      if (ck + 1 < nchunks) {
-        int nxt = FWD ? (chunk + 1) : (chunk - 1);
-        stage_chunk(Ubuf + ((ck + 1) & 1) * (kChunk * kWin), U, ldU, n, R, H, nxt * kChunk);
-      }
+      if (ck + 1 < nchunks)
+        stage_chunk(Ubuf + ((ck + 1) & 1) * (kChunk * kWin), U, ldU, n, R, H,
+                    (FWD ? (chunk + 1) : (chunk - 1)) * kChunk);
       cp_commit();
 
 #pragma unroll 1
       for (int blk = 0; blk < kChunk / 8; ++blk) {
-        // global sweep index of the first sweep of this block
         const int hb = FWD ? (chunk * kChunk + blk * 8) : (chunk * kChunk + kChunk - 1 - blk * 8);
-        const int gblk = ck * (kChunk / 8) + blk;            // running block counter
+        const int gblk = ck * (kChunk / 8) + blk;
         const double* in_cur = inbuf + (gblk & 1) * (8 * kCols);
         double* in_nxt = inbuf + ((gblk + 1) & 1) * (8 * kCols);
         // prefetch the next block's incoming rows
-        double pre;
+        double preA, preB;
         {
           long row = FWD ? (R + hb + 8 + 257 + io_r) : (R + hb - 8 - io_r);
-          pre = (io_col_ok && row < n && row >= 0) ? io_colp[row] : 0.0;
+          const bool rok = row < n && row >= 0;
+          preA = (okA && rok) ? colA[row] : 0.0;
+          preB = (okB && rok) ? colB[row] : 0.0;
         }
-        __syncwarp();
 #pragma unroll
         for (int P = 0; P < 8; ++P) {
           const int h = FWD ? (hb + P) : (hb - P);
-          const int hc = h - chunk * kChunk;
-          const double* us = cur + hc * kWin;
+          const double* us = cur + (h - chunk * kChunk) * kWin;
           double u[8];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) u[j] = us[j * 32 + lane];
+          for (int j = 0; j < 8; ++j) u[j] = us[uslot(lane, j)];
+          double d[kCols];
 #pragma unroll
           for (int c = 0; c < kCols; ++c) {
-            double d = 0.0;
+            double d0 = 0.0, d1 = 0.0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const int pj = FWD ? ((j + P) & 7) : ((j - P) & 7);
-              d = fma(u[j], x[c][pj], d);
+            for (int j = 0; j < 8; j += 2) {
+              d0 = fma(u[j], x[c][FWD ? ((j + P) & 7) : ((j - P) & 7)], d0);
+              d1 = fma(u[j + 1], x[c][FWD ? ((j + 1 + P) & 7) : ((j + 1 - P) & 7)], d1);
             }
-            d += __shfl_xor_sync(0xffffffffu, d, 1);
-            d += __shfl_xor_sync(0xffffffffu, d, 2);
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const int pj = FWD ? ((j + P) & 7) : ((j - P) & 7);
-              x[c][pj] = fma(-d, u[j], x[c][pj]);
-            }
+            d[c] = d0 + d1;
           }
-          // slide the window by one row
-          if (FWD) {
-            // logical row 0 (physical P) leaves at lane 0; lane l takes lane l+1's
 #pragma unroll
-            for (int c = 0; c < kCols; ++c) {
-              double outv = x[c][P & 7];
-              double nv = __shfl_down_sync(0xffffffffu, outv, 1);
-              if (lane == 0) outbuf[P * kCols + c] = outv;
-              if (lane == 31) nv = in_cur[P * kCols + c];
-              x[c][P & 7] = nv;
-            }
-          } else {
-            // logical row 7 (physical (7-P)&7) leaves at lane 31; lane l takes lane l-1's
+          for (int c = 0; c < kCols; ++c) d[c] += __shfl_xor_sync(0xffffffffu, d[c], 1);
 #pragma unroll
-            for (int c = 0; c < kCols; ++c) {
-              const int pp = (7 - P) & 7;
-              double outv = x[c][pp];
-              double nv = __shfl_up_sync(0xffffffffu, outv, 1);
-              if (lane == 31) outbuf[P * kCols + c] = outv;
-              if (lane == 0) nv = in_cur[P * kCols + c];
-              x[c][pp] = nv;
+          for (int c = 0; c < kCols; ++c) d[c] += __shfl_xor_sync(0xffffffffu, d[c], 2);
+#pragma unroll
+          for (int c = 0; c < kCols; ++c)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int pj = FWD ? ((j + P) & 7) : ((j - P) & 7);
+              x[c][pj] = fma(-d[c], u[j], x[c][pj]);
             }
+          // slide the window by one row (register ring, phase P is a constant):
+          // FWD: logical row 0 (physical P) leaves through lane 0 and every lane
+          //      takes lane l+1's; REV: logical row 7 (physical (7-P)&7) leaves
+          //      through lane 31 and every lane takes lane l-1's.  The rotation
+          //      hands the leaving value to the lane that receives the new row.
+          const int pp = FWD ? (P & 7) : ((7 - P) & 7);
+          const int src = FWD ? ((lane + 1) & 31) : ((lane + 31) & 31);
+          const bool edge = FWD ? (lane == 31) : (lane == 0);
+#pragma unroll
+          for (int c = 0; c < kCols; ++c) {
+            const double t = __shfl_sync(0xffffffffu, x[c][pp], src);
+            const double inv = in_cur[P * kCols + c];
+            if (edge) outbuf[P * kCols + c] = t;
+            x[c][pp] = edge ? inv : t;
           }
         }
         __syncwarp();
         // write back the 8 rows that left the window, stage the next incoming rows
         {
-          // FWD: rows R+hb+1+r ; REV: rows R+hb+256-r
           long row = FWD ? (R + hb + 1 + io_r) : (R + hb + 256 - io_r);
-          if (io_col_ok && row < n) io_colp[row] = outbuf[io_r * kCols + io_c];
-          in_nxt[io_r * kCols + io_c] = pre;
+          if (row < n) {
+            if (okA) colA[row] = outbuf[io_r * kCols + io_c];
+            if (okB) colB[row] = outbuf[io_r * kCols + io_c + 4];
+          }
+          in_nxt[io_r * kCols + io_c] = preA;
+          in_nxt[io_r * kCols + io_c + 4] = preB;
         }
         __syncwarp();
       }
     }
-    // ---- write back the final window ----
     // Every sweep is followed by a one-row slide and Hp % 8 == 0 (phase back
     // to 0): FWD ends with the window at R+Hp+1, REV at R (one above sweep 0's).
     const long wsf = FWD ? (R + Hp + 1) : R;

@@ -199,11 +199,19 @@ __global__ void __launch_bounds__(kChaseThreads)
         }
       }
       __syncthreads();
-      // the previous tile (S2 of the last step + this B1) is now final
+      // the previous tile (S2 of the last step + this B1) is now final: store
+      // it and publish progress right away.  A successor may then read
+      // columns < prog - 32 = r, i.e. exactly what has been stored; this
+      // step's S2 and B1' (columns >= r) are not needed by it yet, so the
+      // updates below stay off the inter-sweep critical path.
       tile_store(sub, P, r - cb, cb);
       // (4) this thread's copies of T are done; the barrier makes all visible
       cp_async_commit_wait_all();
       __syncthreads();
+      if (rb2 > 1 && tid == 0) {
+        __threadfence();
+        st_release(prog + s, (int)r2);
+      }
 
       // (5) S2 <- H S2 H  with S(i, j) = T[j][i-j] (i >= j)
       {
@@ -259,7 +267,6 @@ __global__ void __launch_bounds__(kChaseThreads)
         cta_publish(prog + s, n + 3 * kBW);
         break;
       }
-      cta_publish(prog + s, (int)r2);
       cb = rb;
       rb = rb2;
       r = r2;

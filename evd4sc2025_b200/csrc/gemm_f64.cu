@@ -36,6 +36,36 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
       : "d"(a), "d"(b));
 }
 
+// m16n8k4: A rows g and g+8 (column t), B row t (column g); D holds
+// (g, 2t), (g, 2t+1), (g+8, 2t), (g+8, 2t+1).
+__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b));
+}
+
+// m16n8k8: A (g, t), (g+8, t), (g, t+4), (g+8, t+4); B (t, g), (t+4, g).
+__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[8],
+                                            const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+// m16n8k16: A (g + 8(q&1), t + 4(q>>1)) for q = 0..7; B (t + 4q, g) for q = 0..3.
+__device__ __forceinline__ void dmma_16x8x16(double (&d)[4], const double (&a)[8],
+                                             const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+      "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+        "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
@@ -109,12 +139,18 @@ __device__ __forceinline__ void load_tile(double* smem, GPtr g, SOff s_off, int 
   }
 }
 
-template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA>
 __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     dgemm_kernel(const GemmArgs p) {
   constexpr int NWM = BM / WM, NWN = BN / WN;
   constexpr int NT = NWM * NWN * 32;
-  constexpr int MI = WM / 8, NJ = WN / 8;
+  // MMA: 0 = m8n8k4, 1 = m16n8k4, 2 = m16n8k8, 3 = m16n8k16
+  constexpr int MR = (MMA >= 1) ? 16 : 8;  // rows per MMA tile
+  constexpr int NC = (MMA >= 1) ? 4 : 2;   // accumulators per lane per MMA tile
+  constexpr int KS = (MMA == 3) ? 16 : ((MMA == 2) ? 8 : 4);  // k per MMA
+  constexpr int NA = (MMA == 3) ? 8 : ((MMA == 2) ? 4 : ((MMA == 1) ? 2 : 1));
+  constexpr int NB = KS / 4;
+  constexpr int MI = WM / MR, NJ = WN / 8;
   using AT = ATile<TA, BM, BK>;
   using BT = BTile<TB, BN, BK>;
 
@@ -167,11 +203,13 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   const int wm0 = (warp % NWM) * WM, wn0 = (warp / NWM) * WN;
   const int g = lane >> 2, t = lane & 3;
 
-  double acc[MI][NJ][2];
+  double acc[MI][NJ][NC];
 #pragma unroll
   for (int i = 0; i < MI; ++i)
 #pragma unroll
-    for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int h = 0; h < NC; ++h) acc[i][j][h] = 0.0;
 
   auto issue = [&](int kt, int stage) {
     const int k0 = kbeg + kt * BK;
@@ -192,7 +230,12 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
           [&](int ci, int si) { return AT::at(ci, si); }, mlim, klim, p.vecA, p.A);
     } else {
       load_tile<BK, BM, NT>(
-          as, [&](int ci, int si) { return Ab + (long)(k0 + ci) + (long)(m0 + si) * p.lda; },
+          as,
+          [&](int ci, int si) {
+            int mg = m0 + si;
+            if (mg < p.m1) return Ab + (long)(k0 + ci) + (long)mg * p.lda;
+            return p.Am2 + (long)(k0 + ci) + (long)(mg - p.m1) * p.ldam2;
+          },
           [&](int ci, int si) { return AT::at(si, ci); }, klim, mlim, p.vecA, p.A);
     }
     if (!TB) {
@@ -228,16 +271,27 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
     const double* as = As + (kt % STAGES) * AT::kSize;
     const double* bs = Bs + (kt % STAGES) * BT::kSize;
 #pragma unroll
-    for (int kk = 0; kk < BK; kk += 4) {
-      double a[MI], b[NJ];
-#pragma unroll
-      for (int i = 0; i < MI; ++i) a[i] = as[AT::at(wm0 + i * 8 + g, kk + t)];
-#pragma unroll
-      for (int j = 0; j < NJ; ++j) b[j] = bs[BT::at(kk + t, wn0 + j * 8 + g)];
+    for (int kk = 0; kk < BK; kk += KS) {
+      double a[MI][8], b[NJ][4];
 #pragma unroll
       for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        for (int q = 0; q < NA; ++q)
+          a[i][q] = as[AT::at(wm0 + i * MR + g + 8 * (q & 1), kk + t + 4 * (q >> 1))];
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int q = 0; q < NB; ++q) b[j][q] = bs[BT::at(kk + t + 4 * q, wn0 + j * 8 + g)];
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          double(&dd)[4] = *reinterpret_cast<double(*)[4]>(&acc[i][j][0]);
+          if (MMA == 3) dmma_16x8x16(dd, a[i], b[j]);
+          else if (MMA == 2) dmma_16x8x8(dd, a[i], b[j]);
+          else if (MMA == 1) dmma_16x8x4(dd, a[i][0], a[i][1], b[j][0]);
+          else dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i][0], b[j][0]);
+        }
     }
   }
   cp_async_wait<0>();
@@ -250,8 +304,8 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
 #pragma unroll
       for (int j = 0; j < NJ; ++j)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          int r = m0 + wm0 + i * 8 + g, c = n0 + wn0 + j * 8 + 2 * t + h;
+        for (int h = 0; h < NC; ++h) {
+          int r = m0 + wm0 + i * MR + g + 8 * (h >> 1), c = n0 + wn0 + j * 8 + 2 * t + (h & 1);
           if (r < p.m && c < p.n) W[r + (long)c * p.m] = acc[i][j][h];
         }
     return;
@@ -263,8 +317,8 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
 #pragma unroll
     for (int j = 0; j < NJ; ++j)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        int r = m0 + wm0 + i * 8 + g, c = n0 + wn0 + j * 8 + 2 * t + h;
+      for (int h = 0; h < NC; ++h) {
+        int r = m0 + wm0 + i * MR + g + 8 * (h >> 1), c = n0 + wn0 + j * 8 + 2 * t + (h & 1);
         if (r >= p.m || c >= p.n) continue;
         if (mirror && r < c) continue;
         double* dst = Cb + r + (long)c * p.ldc;
@@ -295,12 +349,12 @@ __global__ void dgemm_splitk_reduce_kernel(int m, int n, int splits, long batch_
   }
 }
 
-template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES>
+template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA = 0>
 int launch_cfg(GemmArgs p, int grid_x, int grid_y, cudaStream_t st) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr size_t smem =
       STAGES * (ATile<TA, BM, BK>::kSize + BTile<TB, BN, BK>::kSize) * sizeof(double);
-  auto kern = dgemm_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES>;
+  auto kern = dgemm_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>;
   static bool attr_set = false;  // per instantiation; set once per process
   if (!attr_set) {
     EVD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -357,7 +411,9 @@ static bool aligned16_all(const double* ptr, long ld, long stride) {
 static int gemm_run(GemmArgs p, bool ta, bool tb, long batch, cudaStream_t st,
                     double* ws, size_t ws_doubles) {
   if (p.m <= 0 || p.n <= 0 || batch <= 0) return EVD_SUCCESS;
-  p.vecA = aligned16_all(p.A, p.lda, p.sA) && (p.A2 == nullptr || aligned16(p.A2, p.lda2));
+  p.vecA = aligned16_all(p.A, p.lda, p.sA) && (p.A2 == nullptr || aligned16(p.A2, p.lda2)) &&
+           (p.Am2 == nullptr || aligned16(p.Am2, p.ldam2));
+  if (p.Am2 == nullptr || p.m1 <= 0) p.m1 = p.m;
   p.vecB = aligned16_all(p.B, p.ldb, p.sB) && (p.B2 == nullptr || aligned16(p.B2, p.ldb2));
   if (p.k1 <= 0 || p.A2 == nullptr) p.k1 = p.k;
   if (p.k <= 0) p.splitk = 1;
@@ -489,6 +545,41 @@ int dgemm_nt_pair(long m, long n, long k1, long k2, double alpha, const double* 
   p.mode = kGemm;
   p.splitk = (splitk > 0) ? splitk : choose_splitk(m, n, k1 + k2, 1);
   return gemm_run(p, false, true, 1, st, ws, ws_doubles);
+}
+
+int dgemm_pair(const GemmPair& g, cudaStream_t st, int splitk, double* ws, size_t ws_doubles) {
+  const bool ta = is_trans(g.ta), tb = is_trans(g.tb);
+  if (g.m < 0 || g.n < 0 || g.k < 0) return EVD_ERR_INVALID_ARG;
+  if (g.m == 0 || g.n == 0) return EVD_SUCCESS;
+  if (!g.C || g.ldc < g.m) return EVD_ERR_INVALID_ARG;
+  if (g.Am2 && (!ta || g.m1 <= 0 || g.m1 > g.m)) return EVD_ERR_INVALID_ARG;
+  if (g.A2 && (ta || g.k1 <= 0 || g.k1 > g.k)) return EVD_ERR_INVALID_ARG;
+  if (g.B2 && (!tb || !g.A2)) return EVD_ERR_INVALID_ARG;
+  if (g.m > INT32_MAX || g.n > INT32_MAX || g.k > INT32_MAX) return EVD_ERR_INVALID_ARG;
+  GemmArgs p{};
+  p.m = (int)g.m;
+  p.n = (int)g.n;
+  p.k = (int)g.k;
+  p.alpha = g.alpha;
+  p.beta = g.beta;
+  p.A = g.A ? g.A : g.C;
+  p.lda = g.lda;
+  p.B = g.B ? g.B : g.C;
+  p.ldb = g.ldb;
+  p.C = g.C;
+  p.ldc = g.ldc;
+  p.A2 = g.A2;
+  p.lda2 = g.lda2;
+  p.k1 = g.A2 ? (int)g.k1 : 0;
+  p.B2 = g.B2 ? g.B2 : (g.A2 ? p.B : nullptr);
+  p.ldb2 = g.B2 ? g.ldb2 : g.ldb;
+  if (g.A2 && !g.B2 && tb) return EVD_ERR_INVALID_ARG;
+  p.Am2 = g.Am2;
+  p.ldam2 = g.ldam2;
+  p.m1 = g.Am2 ? (int)g.m1 : 0;
+  p.mode = kGemm;
+  p.splitk = (splitk > 0) ? splitk : choose_splitk(g.m, g.n, g.k, 1);
+  return gemm_run(p, ta, tb, 1, st, ws, ws_doubles);
 }
 
 int syr2k_lower_mirror(long n, long k, double alpha, const double* A, long lda,

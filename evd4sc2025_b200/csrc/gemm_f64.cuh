@@ -22,6 +22,10 @@ struct GemmArgs {
   const double* B2;
   long ldb2;
   int k1;
+  // second A along M (transposed A only): rows m >= m1 of op(A) come from Am2
+  const double* Am2;
+  long ldam2;
+  int m1;
   int mode;
   int splitk;
   double* ws;  // split-K partials: batch * splitk * m * n doubles
@@ -54,6 +58,32 @@ int dgemm_nt_pair(long m, long n, long k1, long k2, double alpha, const double* 
                   const double* B1, long ldb1, const double* A2, long lda2, const double* B2,
                   long ldb2, double beta, double* C, long ldc, cudaStream_t st, int splitk = 1,
                   double* ws = nullptr, size_t ws_doubles = 0);
+
+// General two-operand form used by the ZY update:
+//   op(A) = [A ; Am2] stacked along M (ta == 't' only, split at m1), and/or
+//   op(A) = [A , A2] along K (ta == 'n' only, split at k1; B spans all of K,
+//   or, when tb == 't', B is [B , B2] along K as well).
+struct GemmPair {
+  char ta, tb;
+  long m, n, k;
+  double alpha, beta;
+  const double* A;
+  long lda;
+  const double* B;
+  long ldb;
+  double* C;
+  long ldc;
+  const double* A2 = nullptr;
+  long lda2 = 0;
+  long k1 = 0;
+  const double* B2 = nullptr;
+  long ldb2 = 0;
+  const double* Am2 = nullptr;
+  long ldam2 = 0;
+  long m1 = 0;
+};
+int dgemm_pair(const GemmPair& g, cudaStream_t st, int splitk = 0, double* ws = nullptr,
+               size_t ws_doubles = 0);
 
 // C(lower) = alpha*(A B^T + B A^T) + beta*C(lower); upper = mirror of lower.
 int syr2k_lower_mirror(long n, long k, double alpha, const double* A, long lda,

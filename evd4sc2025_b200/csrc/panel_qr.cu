@@ -145,16 +145,25 @@ __device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, Ti
     double uv[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) uv[i] = sm.us[lane + 32 * i];
+    // the four column dot products are reduced together (interleaved
+    // butterflies); columns <= j get a zero update
+    double pc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      if (4 * warp + c > j) {
-        double p = 0.0;
+      double p = 0.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) p = fma(uv[i], a[c][i], p);
-        double dot = warp_sum(p);
+      for (int i = 0; i < 4; ++i) p = fma(uv[i], a[c][i], p);
+      pc[c] = p;
+    }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
-      }
+    for (int m = 16; m > 0; m >>= 1)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) pc[c] += __shfl_xor_sync(0xffffffffu, pc[c], m);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double dot = (4 * warp + c > j) ? pc[c] : 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
     }
     __syncthreads();
   }
@@ -177,16 +186,23 @@ __device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, Ti
     double uv[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
+    double pc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      if (4 * warp + c >= j) {
-        double p = 0.0;
+      double p = 0.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) p = fma(uv[i], q[c][i], p);
-        double dot = warp_sum(p);
+      for (int i = 0; i < 4; ++i) p = fma(uv[i], q[c][i], p);
+      pc[c] = p;
+    }
 #pragma unroll
-        for (int i = 0; i < 4; ++i) q[c][i] = fma(-dot, uv[i], q[c][i]);
-      }
+    for (int m = 16; m > 0; m >>= 1)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) pc[c] += __shfl_xor_sync(0xffffffffu, pc[c], m);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double dot = (4 * warp + c >= j) ? pc[c] : 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) q[c][i] = fma(-dot, uv[i], q[c][i]);
     }
   }
 #pragma unroll
@@ -301,7 +317,7 @@ __device__ void path_product(const TsqrPlan& plan, const double* ws, int t, Fini
 // mode 0: write the explicit thin Q into A (evd_tsqr).
 // mode 1: write Y (into Yout), W (into Wout), and optionally the band panel
 //         (R over zeros) into Aband (sy2sb).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 1)
     tsqr_finish_kernel(const TsqrPlan plan, const double* ws, double* A, long lda, int mode,
                        double* Yout, long ldy, double* Wout, long ldw, const double* Rin,
                        long ldr, double* Aband, long ldband) {
@@ -313,16 +329,18 @@ __global__ void __launch_bounds__(kThreads)
   const int r0 = t * kTile;
   const int mm = min(kTile, plan.m - r0);
 
-  // tile rows of Q = Qleaf_t * M_t
-  path_product(plan, ws, t, sm);
+  // tile rows of Q = Qleaf_t * M_t; the leaf Q tile is staged in shared
+  // memory (coalesced) before the product
+  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
+    int r = e & (kTile - 1), c = e >> 7;
+    Ws[r * 33 + c] = (r < mm) ? __ldcg(A + (long)(r0 + r) + (long)c * lda) : 0.0;
+  }
+  path_product(plan, ws, t, sm);  // ends with __syncthreads
   for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
     int r = e & (kTile - 1), c = e >> 7;
     double s = 0.0;
-    if (r < mm) {
-      const double* qr = A + (long)(r0 + r);
 #pragma unroll 8
-      for (int k = 0; k < kNB; ++k) s = fma(__ldcg(qr + (long)k * lda), sm.M[k * 33 + c], s);
-    }
+    for (int k = 0; k < kNB; ++k) s = fma(Ws[r * 33 + k], sm.M[k * 33 + c], s);
     Qs[r * 33 + c] = s;
   }
   __syncthreads();

@@ -486,20 +486,21 @@ __global__ void merge_copy_deflated_kernel(LevelArgs a) {
 
 // f(tau) = 1/rho + sum_k z_k^2 / (Delta_k - tau), with Delta_k = d_k - d_o.
 // Root j in (d_j, d_{j+1}) (or (d_{K-1}, d_{K-1} + rho z^T z) for the last).
-__device__ void secular_root(int K, int j, const double* dK, const double* zK, double rho,
-                             double* tau_out, int* org_out) {
+// One warp per root: the lanes split the K terms and every sum is reduced
+// across the warp, so the iteration control is uniform.
+__device__ void secular_root_warp(int K, int j, const double* dK, const double* zK, double rho,
+                                  double* tau_out, int* org_out) {
+  const int lane = threadIdx.x & 31;
   const double dj = dK[j];
   const bool last = (j == K - 1);
-  double zz = 0.0;
-  if (last)
-    for (int k = 0; k < K; ++k) zz = fma(zK[k], zK[k], zz);
   int o;
   double lo_b, hi_b, tau;
   if (!last) {
     const double gap = dK[j + 1] - dj;
     const double mid = 0.5 * gap;
-    double f = 1.0 / rho;
-    for (int k = 0; k < K; ++k) f += zK[k] * zK[k] / ((dK[k] - dj) - mid);
+    double f = 0.0;
+    for (int k = lane; k < K; k += 32) f += zK[k] * zK[k] / ((dK[k] - dj) - mid);
+    f = warp_sum(f) + 1.0 / rho;
     if (f >= 0.0) {  // root in (d_j, d_j + gap/2]
       o = j;
       lo_b = 0.0;
@@ -512,6 +513,9 @@ __device__ void secular_root(int K, int j, const double* dK, const double* zK, d
       tau = -0.5 * mid;
     }
   } else {
+    double zz = 0.0;
+    for (int k = lane; k < K; k += 32) zz = fma(zK[k], zK[k], zz);
+    zz = warp_sum(zz);
     o = j;
     lo_b = 0.0;
     hi_b = rho * zz;
@@ -519,17 +523,25 @@ __device__ void secular_root(int K, int j, const double* dK, const double* zK, d
   }
   const double d_o = dK[o];
   // poles adjacent to the root, relative to the origin
-  const double pl = (o == j) ? 0.0 : (dj - d_o);                 // left pole (index j)
+  const double pl = (o == j) ? 0.0 : (dj - d_o);                        // left pole (index j)
   const double pr = last ? 0.0 : ((o == j) ? (dK[j + 1] - d_o) : 0.0);  // right pole (j+1)
   for (int it = 0; it < 64; ++it) {
     double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0, erret = 0.0;
-    for (int k = 0; k < K; ++k) {
-      double del = (dK[k] - d_o) - tau;
-      double q = zK[k] / del;
-      double term = zK[k] * q;
-      if (k <= j) { psi += term; dpsi += q * q; }
-      else { phi += term; dphi += q * q; }
+    for (int k = lane; k < K; k += 32) {
+      const double del = (dK[k] - d_o) - tau;
+      const double q = zK[k] / del;
+      const double term = zK[k] * q;
+      if (k <= j) { psi += term; dpsi = fma(q, q, dpsi); }
+      else { phi += term; dphi = fma(q, q, dphi); }
       erret += fabs(term);
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+      psi += __shfl_xor_sync(0xffffffffu, psi, m);
+      dpsi += __shfl_xor_sync(0xffffffffu, dpsi, m);
+      phi += __shfl_xor_sync(0xffffffffu, phi, m);
+      dphi += __shfl_xor_sync(0xffffffffu, dphi, m);
+      erret += __shfl_xor_sync(0xffffffffu, erret, m);
     }
     const double f = 1.0 / rho + psi + phi;
     if (f < 0.0) lo_b = fmax(lo_b, tau); else hi_b = fmin(hi_b, tau);
@@ -554,7 +566,6 @@ __device__ void secular_root(int K, int j, const double* dK, const double* zK, d
       if (c == 0.0) eta = C / B;
       else if (B >= 0.0) eta = (B + sq != 0.0) ? 2.0 * C / (B + sq) : 0.0;
       else eta = (B - sq) / (2.0 * c);
-      // pick the root inside (a1, a2) if the chosen one is outside
       if (!(eta > a1 && eta < a2) && c != 0.0) {
         double alt = (B >= 0.0) ? (B + sq) / (2.0 * c) : ((B - sq != 0.0) ? 2.0 * C / (B - sq) : 0.0);
         eta = alt;
@@ -567,43 +578,66 @@ __device__ void secular_root(int K, int j, const double* dK, const double* zK, d
     }
     double tn = tau + eta;
     if (!(tn > lo_b && tn < hi_b) || !isfinite(tn)) tn = 0.5 * (lo_b + hi_b);
-    if (tn == tau) break;
+    if (tn == tau || fabs(tn - tau) <= 2.0 * kEps * fabs(tau)) {
+      tau = tn;
+      break;
+    }
     tau = tn;
   }
   *tau_out = tau;
   *org_out = o;
 }
 
+// grid (ceil(Kmax*32/256), nm), block 256: one warp per root
 __global__ void merge_secular_kernel(LevelArgs a) {
   const int m = blockIdx.y;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long lo = (long)m * a.N;
   const int K = a.desc[8 * m + D_K];
   if (j >= K) return;
   double tau;
   int o;
-  secular_root(K, j, a.dK + lo, a.zK + lo, a.rho[m], &tau, &o);
-  a.tau[lo + j] = tau;
-  a.org[lo + j] = o;
+  secular_root_warp(K, j, a.dK + lo, a.zK + lo, a.rho[m], &tau, &o);
+  if ((threadIdx.x & 31) == 0) {
+    a.tau[lo + j] = tau;
+    a.org[lo + j] = o;
+  }
 }
 
-// z_hat_i^2 = -(d_i - lambda_i) prod_{j != i} (d_i - lambda_j) / (d_i - d_j)
+// z_hat_i^2 = -(d_i - lambda_i) prod_{j != i} (d_i - lambda_j) / (d_i - d_j).
+// One warp per i; each lane keeps its partial product as mantissa * 2^e so
+// that no partial product over- or underflows.
 __global__ void merge_loewner_kernel(LevelArgs a) {
   const int m = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   const long lo = (long)m * a.N;
   const int K = a.desc[8 * m + D_K];
   if (i >= K) return;
   const double* dK = a.dK + lo;
   const double di = dK[i];
-  double w = (di - dK[a.org[lo + i]]) - a.tau[lo + i];
-  for (int j = 0; j < K; ++j) {
-    if (j == i) continue;
-    double delta = (di - dK[a.org[lo + j]]) - a.tau[lo + j];
-    w *= delta / (di - dK[j]);
+  double w = 1.0;
+  int ex = 0;
+  for (int j = lane; j < K; j += 32) {
+    const double delta = (di - dK[a.org[lo + j]]) - a.tau[lo + j];
+    w *= (j == i) ? delta : delta / (di - dK[j]);
+    int e2;
+    w = frexp(w, &e2);
+    ex += e2;
   }
-  double z = sqrt(fmax(0.0, -w));
-  a.zh[lo + i] = (a.zK[lo + i] >= 0.0) ? z : -z;
+#pragma unroll
+  for (int mm = 16; mm > 0; mm >>= 1) {
+    const double ow = __shfl_xor_sync(0xffffffffu, w, mm);
+    const int oe = __shfl_xor_sync(0xffffffffu, ex, mm);
+    int e2;
+    w = frexp(w * ow, &e2);
+    ex += oe + e2;
+  }
+  if (lane == 0) {
+    const double wv = ldexp(w, ex);
+    const double z = sqrt(fmax(0.0, -wv));
+    a.zh[lo + i] = (a.zK[lo + i] >= 0.0) ? z : -z;
+  }
 }
 
 // U(:, j): v_i = zhat_i / (d_i - lambda_j), normalised; rows placed in the
@@ -830,10 +864,10 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     merge_gather_kernel<<<gN, 256, 0, st>>>(a);
     EVD_LAUNCHED();
     if (Kmax > 0) {
-      dim3 gK(ceil_div_i(Kmax, 128), a.nm);
-      merge_secular_kernel<<<gK, 128, 0, st>>>(a);
+      dim3 gK(ceil_div_i((long)Kmax * 32, 256), a.nm);
+      merge_secular_kernel<<<gK, 256, 0, st>>>(a);
       EVD_LAUNCHED();
-      merge_loewner_kernel<<<gK, 128, 0, st>>>(a);
+      merge_loewner_kernel<<<gK, 256, 0, st>>>(a);
       EVD_LAUNCHED();
       merge_vectors_kernel<<<dim3(Kmax, a.nm), 256, 0, st>>>(a);
       EVD_LAUNCHED();

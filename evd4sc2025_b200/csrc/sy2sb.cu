@@ -12,7 +12,9 @@
 // B200 differences (same arithmetic, fewer passes):
 //  * the panel kernel writes Y -> dY, W -> dW and the band panel (R over
 //    zeros) -> dA directly (no copyMatrix / getU kernels);
-//  * the lazy update is ONE two-operand-pair GEMM (K = 2i) instead of two;
+//  * the lazy update is ONE two-operand-pair GEMM (K = 2i) instead of two, and
+//    likewise Z_prev^T W / Y_prev^T W (one GEMM stacked along M) and the two
+//    corrections of Z (one GEMM with K = 2(i-b));
 //  * the trailing SYR2K computes lower tiles only and its epilogue mirrors them
 //    (no separate copyMatrixL2U pass);
 //  * instead of copying the whole trailing matrix OA -> dA after each frame
@@ -68,7 +70,7 @@ static Sy2sbLayout sy2sb_layout(long M, long b, long nb) {
   Sy2sbLayout L{};
   L.panel_off = 0;
   L.panel_n = panel_qr_ws_doubles(M);
-  L.small_n = nb * b;
+  L.small_n = 2 * nb * b;  // [S1; S2] is 2kp x b
   L.s1_off = L.panel_off + L.panel_n;
   L.s2_off = L.s1_off + L.small_n;
   L.s3_off = L.s2_off + L.small_n;
@@ -123,12 +125,18 @@ int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, lo
         const long kp = i - b;
         const double* Zprev = dZ + i;             // rows i.., cols 0..kp-1
         const double* Yprev = dY + g0 + off * ldY;
-        // S1 = Zprev^T W ; S2 = Yprev^T W   (kp x b)
-        EVD_TRY(dgemm('t', 'n', kp, b, m, 1.0, Zprev, ldZ, Wp, ldW, 0.0, S1, kp, st, 0, SK, skn));
-        EVD_TRY(dgemm('t', 'n', kp, b, m, 1.0, Yprev, ldY, Wp, ldW, 0.0, S2, kp, st, 0, SK, skn));
-        // Z -= Yprev S1 + Zprev S2
-        EVD_TRY(dgemm('n', 'n', m, b, kp, -1.0, Yprev, ldY, S1, kp, 1.0, Zp, ldZ, st, 0, SK, skn));
-        EVD_TRY(dgemm('n', 'n', m, b, kp, -1.0, Zprev, ldZ, S2, kp, 1.0, Zp, ldZ, st, 0, SK, skn));
+        // [S1; S2] = [Zprev | Yprev]^T W  (2kp x b, one GEMM stacked along M)
+        GemmPair g1{'t', 'n', 2 * kp, b, m, 1.0, 0.0, Zprev, ldZ, Wp, ldW, S1, 2 * kp};
+        g1.Am2 = Yprev;
+        g1.ldam2 = ldY;
+        g1.m1 = kp;
+        EVD_TRY(dgemm_pair(g1, st, 0, SK, skn));
+        // Z -= [Yprev, Zprev] [S1; S2]  (one GEMM, operands switched at K = kp)
+        GemmPair g2{'n', 'n', m, b, 2 * kp, -1.0, 1.0, Yprev, ldY, S1, 2 * kp, Zp, ldZ};
+        g2.A2 = Zprev;
+        g2.lda2 = ldZ;
+        g2.k1 = kp;
+        EVD_TRY(dgemm_pair(g2, st, 0, SK, skn));
       }
       // Z -= 1/2 Y (W^T Z)
       EVD_TRY(dgemm('t', 'n', b, b, m, 1.0, Wp, ldW, Zp, ldZ, 0.0, S3, b, st, 0, SK, skn));
