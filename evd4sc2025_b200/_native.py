@@ -36,6 +36,7 @@ SIGNATURES = {
     "evd_band_pack": (_i, [_l, _l, _p, _l, _p, _l, _p]),
     "evd_bulge_chase_iwork_size": (_l, [_l]),
     "evd_bulge_chase": (_i, [_l, _l, _p, _l, _p, _l, _p, _p, _p, _p]),
+    "evd_bulge_chase_noalloc": (_i, [_l, _l, _p, _l, _p, _l, _p, _p, _p]),
     "evd_stedc_work_size": (_l, [_l]),
     "evd_stedc_iwork_size": (_l, [_l]),
     "evd_stedc": (_i, [_l, _p, _p, _p, _l, _p, _l, _p, _l, _p]),

@@ -28,6 +28,8 @@
 //    row/column, two shuffle steps per dot product).
 //  * every wait is bounded in time; on timeout the kernel records an error
 //    word, all CTAs drain, and the host returns EVD_ERR_TIMEOUT.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace evd {
@@ -369,4 +371,68 @@ extern "C" int evd_bulge_chase(long n, long b, double* dSub, long ldSub, double*
   int rc = evd::bulge_chase_async(n, b, dSub, ldSub, dU, ldU, d, e, iwork, stream);
   if (rc != EVD_SUCCESS || n <= 2) return rc;
   return evd::read_device_error(iwork + n + 32, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the bulge chasing entry point.
+//
+// evd_bulge_chase needs a small integer scratch buffer (progress flags of the
+// sweeps, the sweep ticket and an error word) and takes it from the caller.
+// Some callers have no way to obtain device memory at the point where they
+// run the chase: code that must not call cudaMalloc (it can synchronise the
+// whole device, fail under memory pressure, or is simply unavailable to a
+// plugin running inside a host framework that owns the allocator), and
+// loops that are required to run with a fixed memory footprint.  For them the
+// scratch lives in a file-scope device array instead, sized for bands of up
+// to kNoAllocMaxN columns (256 KB that every GPU loading this library keeps
+// until the process exits).
+namespace evd {
+
+constexpr long kNoAllocMaxN = 65536;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) int g_chase_noalloc_scratch[kNoAllocMaxN + 64];
+
+// Device address of the scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up with
+// cudaGetSymbolAddress, once per device (with that device current), and cached.
+static int chase_noalloc_scratch(int** out) {
+  static std::mutex mu;
+  static int* addr[kNoAllocMaxDevices] = {};
+  int dev = 0;
+  EVD_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return EVD_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&p, g_chase_noalloc_scratch);
+    if (rc != cudaSuccess || p == nullptr) {
+      fprintf(stderr, "evd_b200: cudaGetSymbolAddress for the chase scratch failed: %s\n",
+              cudaGetErrorString(rc));
+      return EVD_ERR_CUDA;
+    }
+    addr[dev] = static_cast<int*>(p);
+  }
+  *out = addr[dev];
+  return EVD_SUCCESS;
+}
+
+}  // namespace evd
+
+extern "C" int evd_bulge_chase_noalloc(long n, long b, double* dSub, long ldSub, double* dU,
+                                       long ldU, double* d, double* e, cudaStream_t stream) {
+  if (n > evd::kNoAllocMaxN) {
+    fprintf(stderr,
+            "evd_b200: evd_bulge_chase_noalloc supports n <= %ld (got n = %ld); use "
+            "evd_bulge_chase with a caller-provided scratch buffer\n",
+            evd::kNoAllocMaxN, n);
+    return EVD_ERR_INVALID_ARG;
+  }
+  int* iw = nullptr;
+  EVD_TRY(evd::chase_noalloc_scratch(&iw));
+  // bulge_chase_async clears the flags, ticket and error word of the scratch
+  // (cudaMemsetAsync) before every launch, so a call never sees stale state.
+  int rc = evd::bulge_chase_async(n, b, dSub, ldSub, dU, ldU, d, e, iw, stream);
+  if (rc != EVD_SUCCESS || n <= 2) return rc;
+  return evd::read_device_error(iw + n + 32, stream);
 }

@@ -132,6 +132,20 @@ long evd_bulge_chase_iwork_size(long n);
 int evd_bulge_chase(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
                     double* d, double* e, int* iwork, cudaStream_t stream);
 
+/* Same as evd_bulge_chase, but allocates nothing and takes no scratch: for
+ * callers that cannot obtain device memory where they run the chase (no
+ * cudaMalloc allowed there: a fixed memory footprint, or a host framework that
+ * owns the allocator).  This entry point has no counterpart in the reference.
+ * Its scratch is a file-scope device array of the library, sized for
+ * n <= 65536 (256 KB per GPU that loads the library, kept until exit); larger
+ * n is rejected with EVD_ERR_INVALID_ARG and a message on stderr.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the one
+ * array and clears it first, so calls that overlap on the GPU (other streams,
+ * other host threads) race: serialise them.  Synchronises `stream`. */
+int evd_bulge_chase_noalloc(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
+                            double* d, double* e, cudaStream_t stream);
+
 /* ---- Tridiagonal eigensolver (device divide and conquer) ---------------- */
 
 long evd_stedc_work_size(long n);   /* doubles */
