@@ -248,12 +248,21 @@ def bc_back(Q: torch.Tensor, U: torch.Tensor, b: int = 32, stream=None) -> torch
 my_BC_back_trans_v8_10_noBandU = bc_back
 
 
-def bc_back_apply(X: torch.Tensor, U: torch.Tensor, b: int = 32, stream=None) -> torch.Tensor:
-    """X <- Q2 X (in place): the chasing reflectors in reverse generation order."""
+def bc_back_apply(X: torch.Tensor, U: torch.Tensor, b: int = 32, stream=None,
+                  work: torch.Tensor | bool | None = True) -> torch.Tensor:
+    """X <- Q2 X (in place): the chasing reflectors in reverse generation order.
+
+    ``work``: a float64 CUDA tensor of at least evd_bc_back_work_size(n)
+    elements for the precomputed T factors, True to allocate one here, or
+    None to let the kernel rebuild them (no workspace).
+    """
     n, ncols = X.shape
     px, ldx = _cm(X, "X")
     pu, ldu = _cm(U, "U")
-    call("evd_bc_back_apply", n, ncols, pu, ldu, px, ldx, b, _stream(stream))
+    if work is True:
+        work = torch.empty(max(1, lib().evd_bc_back_work_size(n)), dtype=F64, device=X.device)
+    pw, lw = (None, 0) if work is None else (_ptr(work), work.numel())
+    call("evd_bc_back_apply", n, ncols, pu, ldu, px, ldx, b, pw, lw, _stream(stream))
     return X
 
 

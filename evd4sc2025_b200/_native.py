@@ -41,7 +41,8 @@ SIGNATURES = {
     "evd_stedc_iwork_size": (_l, [_l]),
     "evd_stedc": (_i, [_l, _p, _p, _p, _l, _p, _l, _p, _l, _p]),
     "evd_bc_back": (_i, [_p, _l, _p, _l, _l, _i, _p]),
-    "evd_bc_back_apply": (_i, [_l, _l, _p, _l, _p, _l, _i, _p]),
+    "evd_bc_back_work_size": (_l, [_l]),
+    "evd_bc_back_apply": (_i, [_l, _l, _p, _l, _p, _l, _i, _p, _l, _p]),
     "evd_wy_from_slide": (_i, [_l, _l, _l, _p, _l, _p, _l, _p, _p]),
     "evd_q_from_wy": (_i, [_l, _l, _p, _l, _p, _l, _p, _l, _p]),
     "evd_sbr_back_work_size": (_l, [_l, _l, _l]),

@@ -8,38 +8,58 @@
 //             api/BC_backTransV8_10_noBandU.cu:60-313):  X <- Q2^T X
 //   reverse  (evd_bc_back_apply, the eigenvector direction): X <- Q2 X
 //
-// Ordering.  Rows are cut into 256-row strips R = 0, 256, ...  In strip R
-// sweep h touches exactly rows [R+h+1, R+h+257) (8 reflectors, k = R/32 ..
-// R/32+7).  Overlapping reflectors of sweeps s < s' must be applied s first
-// (forward) or s' first (reverse); processing strips bottom-up with sweeps
-// ascending (forward), or top-down with sweeps descending (reverse), respects
-// that: the overlap of strip R's sweep h with strip R+-256 occurs only for
-// sweeps on the correct side.  (The reference uses the forward order.)
+// Ordering.  Rows are cut into 128-row strips R = 0, 128, ...  In strip R
+// sweep h touches exactly rows [R+h+1, R+h+129) (4 reflectors, k = R/32 ..
+// R/32+3).  Strips run bottom-up (forward) or top-down (reverse); that
+// respects the generation order because the overlap of strip R's sweep h with
+// strip R+-128 occurs only for sweeps on the correct side.
 //
-// B200 layout (not the reference's): a warp owns 8 columns of X and holds the
-// 256-row window in registers, lane l holding rows 8l..8l+7 of each column,
-// so a 32-row reflector is 4 lanes (2 shuffle steps per dot product, eight
-// independent dot products per sweep) and each reflector value read from
-// shared memory feeds 8 columns.  The window slides one row per sweep through
-// a ring of 8 registers (the phase is a compile-time constant inside an
-// 8-sweep block): one rotation shuffle per column, no register moves, no
-// divergent branches; the row leaving the window is written back and the row
-// entering is prefetched one block ahead.  Reflector chunks (16 sweeps x 256
-// rows) are double-buffered in shared memory with cp.async, in a rotated
-// layout that is bank-conflict free for both the copy and the reads; 4-warp
-// CTAs so that two or more fit per SM.  Exactly 2 n^2 ncols flops, FP64 FMA; rows >= n are never read or
-// written (the reference needs 346 zero rows of padding).
+// Blocking (B200 design, not the reference's).  Inside a strip, sweeps are
+// taken 8 at a time (block bb: sweeps 8bb..8bb+7).  The 8 reflectors of one
+// block on segment j form a "group": they live in the 40-row parallelogram
+// starting at row R+8bb+1+32j, reflector p on rows p..p+31 of it.  Two
+// reflectors of different groups of a block overlap only if their segments
+// are adjacent, and then the one on the lower segment comes first in
+// generation order, so a block is applied group by group from the bottom
+// segment up (forward; top-down and block order reversed for reverse).  A
+// group is applied as one compact-WY update on the FP64 tensor cores:
+//   Y (40 x 8, zero outside the parallelogram), T = (I + striu(Y^T Y))^-1
+//   (unit upper triangular; every stored reflector has tau = 1),
+//   forward X <- X - Y T^T (Y^T X),  reverse X <- X - Y T (Y^T X),
+// as DMMA m16n8k8 products with X^T in the accumulator layout: a warp owns 16
+// columns and keeps the block's 17 x 8-row window in registers; the
+// accumulator layout of an 8-row tile doubles as the A operand of the next
+// product (the k index is permuted to rows 0,2,4,6,1,3,5,7 and the B operand
+// is read with the same permutation), so the window is never shuffled.
+// T (Y^T Y by m8n8k4, then a triangular solve by 8 lanes) is either built by
+// a separate fully parallel kernel into a caller workspace before the apply
+// kernel runs (q2_tbuild_kernel; the apply kernel then stages it with the
+// reflectors), or, without a workspace, built inside the apply kernel one
+// block ahead.  U is staged by cp.async into zero-padded, bank-conflict-free
+// segments three blocks deep.  Work: the
+// 2 n^2 ncols flops of the reflector algebra are done as 2.75 n^2 ncols on
+// the DMMA pipe (parallelogram padding 40/32, plus the T product), plus the
+// Gram products.  Rows >= n are never read or written (the reference needs
+// 346 zero rows of padding).
 #include "common.cuh"
 
 namespace evd {
 
 namespace {
 
-constexpr int kWin = 256;   // window rows (8 reflectors of 32)
-constexpr int kCols = 8;    // columns per warp
-constexpr int kWarps = 4;   // warps per CTA
-constexpr int kChunk = 16;  // sweeps per staged reflector chunk
-constexpr int kThreadsBC = kWarps * 32;
+constexpr int kQW = 4;                   // warps per CTA
+constexpr int kQCols = 16;               // columns per warp (MMA M)
+constexpr int kQThreads = kQW * 32;
+constexpr int kStrip = 128;              // strip height (rows)
+constexpr int kGroups = kStrip / 32;     // segments (groups) per block
+constexpr int kTiles = 4 * kGroups + 1;  // 8-row tiles in a block's window (135 rows used)
+constexpr int kSeg = 64;                 // smem slots per (sweep, segment): 8 + 32 + 8 used
+constexpr int kYBuf = 8 * kGroups * kSeg;  // 8 sweeps x kGroups segments
+constexpr int kNYBuf = 3;
+constexpr int kTBuf = kGroups * 32 * 2;  // per group: 32 lanes x 2 B-fragment values
+constexpr int kGBuf = 64;                // per warp: one 8 x 8 Gram matrix
+constexpr size_t kQSmem = (size_t)(kNYBuf * kYBuf + kNYBuf * kTBuf + kQW * kGBuf) * sizeof(double);
+static_assert(kGroups == kQW, "one warp builds the T of one group");
 
 __device__ __forceinline__ void cp_async8_zfill(double* smem, const double* gmem, bool valid) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -48,219 +68,387 @@ __device__ __forceinline__ void cp_async8_zfill(double* smem, const double* gmem
                : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async16(double* smem, const double* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
-// Shared-memory slot of window row i = 8l + j of one staged sweep: lane l reads
-// its 8 values at j*32 + rot(l, j); the rotation by 4j keeps both the staging
-// writes (consecutive rows) and the per-sweep reads (consecutive lanes) free
-// of bank conflicts.
-__device__ __forceinline__ int uslot(int l, int j) { return j * 32 + ((l + 4 * j) & 31); }
+__device__ __forceinline__ void mma16(double (&d)[4], double a0, double a1, double a2, double a3,
+                                      double b0, double b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+__device__ __forceinline__ void mma8(double (&d)[2], double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
+}
 
-// Stage reflectors of sweeps [h0, h0+kChunk) for strip R (zero for h >= H or
-// row >= n): buf[hc*256 + uslot(l, j)] = U(R+h+1 + 8l+j, h).
-__device__ __forceinline__ void stage_chunk(double* buf, const double* U, long ldU, int n, long R,
-                                            int H, int h0) {
-  for (int e = threadIdx.x; e < kChunk * kWin; e += kThreadsBC) {
-    int hc = e >> 8, i = e & 255;
-    int h = h0 + hc;
-    long row = R + h + 1 + i;
-    bool valid = (h < H) && (row < n);
+// Segment (sweep p, segment j) of a staged block: Y_j[r][p] is at
+// seg_off(p, j) + r - p for r - p in [-8, 40) (zero outside [0, 32)).  The
+// offset 10 * ((p >> 1) & 1) makes both fragment read patterns below
+// conflict-free (each half-warp hits 16 distinct 8-byte banks).
+__device__ __forceinline__ int seg_off(int p, int j) {
+  return (p * kGroups + j) * kSeg + 10 * ((p >> 1) & 1) + 8;
+}
+
+// Stage block bb of strip R: Y values of sweeps 8bb..8bb+7 (zero for sweep
+// >= H or row >= n).  Element i of sweep p's strip window goes to segment
+// i / 32, offset i % 32.
+__device__ __forceinline__ void stage_block(double* ys, const double* U, long ldU, int n, long R,
+                                            int H, int bb) {
+  for (int e = threadIdx.x; e < 8 * kStrip; e += kQThreads) {
+    const int p = e / kStrip, i = e % kStrip;
+    const int h = 8 * bb + p;
+    const long row = R + h + 1 + i;
+    const bool valid = (h < H) && (row < n);
     const double* src = valid ? (U + row + (long)h * ldU) : U;
-    cp_async8_zfill(buf + hc * kWin + uslot(i >> 3, i & 7), src, valid);
+    cp_async8_zfill(ys + seg_off(p, i >> 5) + (i & 31), src, valid);
   }
 }
 
+// -T fragment of group w of a staged block (warp w).  G = Y^T Y by DMMA (the
+// Y fragment is both operands), then lane q solves (I + striu(G)) t = e_q for
+// column q of T, and stores -T as the B operand of the W <- W T (forward:
+// B[k][n] = T[k][n]) or W <- W T^T (reverse) product, k permuted as in the
+// window tiles.
 template <bool FWD>
-__global__ void __launch_bounds__(kThreadsBC, 2)
-    q2_apply_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
-                    double* __restrict__ X, long ldX) {
-  extern __shared__ double smem[];
-  double* Ubuf = smem;                                   // 2 x kChunk x kWin
-  double* iobase = smem + 2 * kChunk * kWin;             // per warp: in[2][8][C], out[8][C]
+__device__ __forceinline__ void build_t(const double* ys, double* ts, double* gs, int warp,
+                                        int lane, int offW) {
+  const int j = warp;
+  {
+    double ga[2] = {0.0, 0.0}, gb[2] = {0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const double y0 = ys[offW + j * kSeg + 8 * i];
+      const double y1 = ys[offW + j * kSeg + 8 * i + 1];
+      mma8(ga, y0, y0);
+      mma8(gb, y1, y1);
+    }
+    const int g = lane >> 2, t = lane & 3;
+    gs[g * 8 + 2 * t] = ga[0] + gb[0];
+    gs[g * 8 + 2 * t + 1] = ga[1] + gb[1];
+  }
+  __syncwarp();
+  if (lane < 8) {
+    const int q = lane;
+    const double* G = gs;
+    double tq[8];
+#pragma unroll
+    for (int i = 7; i >= 0; --i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = i + 1; k < 8; ++k) acc = fma(G[i * 8 + k], tq[k], acc);
+      tq[i] = (i < q) ? -acc : (i == q ? 1.0 : 0.0);
+    }
+    double* dst = ts + j * 64;
+    if (FWD) {
+      // lane (g, t) of the product needs T[2t][g], T[2t+1][g]: column g = q
+#pragma unroll
+      for (int t2 = 0; t2 < 4; ++t2) {
+        dst[(4 * q + t2) * 2 + 0] = -tq[2 * t2];
+        dst[(4 * q + t2) * 2 + 1] = -tq[2 * t2 + 1];
+      }
+    } else {
+      // lane (g, t) needs T[g][2t], T[g][2t+1]: row g, columns 2t, 2t+1
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dst[(4 * i + (q >> 1)) * 2 + (q & 1)] = -tq[i];
+    }
+  }
+}
+
+// Blocks of all strips, strip-major: strip s has nblk(s) = B0 - 16 s blocks
+// (B0 = ceil((n-2)/8); every strip height is a multiple of 8 rows), so the T
+// fragments of block bb of strip s start at tblock(s, bb) * kTBuf.
+__host__ __device__ __forceinline__ long tblock(long s, long bb, long B0) {
+  return s * B0 - 8 * s * (s - 1) + bb;
+}
+
+// -T fragments of every block of every strip (one CTA per block, one warp
+// per group), in the layout the apply kernel reads.
+template <bool FWD>
+__global__ void __launch_bounds__(kQThreads)
+    q2_tbuild_kernel(int n, const double* __restrict__ U, long ldU, double* __restrict__ Tg) {
+  __shared__ __align__(16) double ys[kYBuf];
+  __shared__ double gsh[kQW * kGBuf];
+  const int s = blockIdx.y, bb = blockIdx.x;
+  const int B0 = (n - 2 + 7) / 8;
+  const int nblk = B0 - (kStrip / 8) * s;
+  if (bb >= nblk) return;
+  const long R = (long)s * kStrip;
+  const int H = n - 2 - (int)R;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* inbuf = iobase + warp * (3 * 8 * kCols);
-  double* outbuf = inbuf + 2 * 8 * kCols;
-  const int col0 = blockIdx.x * (kWarps * kCols) + warp * kCols;
+  const int g = lane >> 2, t = lane & 3;
+  for (int e = threadIdx.x; e < kYBuf; e += kQThreads) ys[e] = 0.0;
+  __syncthreads();
+  stage_block(ys, U, ldU, n, R, H, bb);
+  cp_commit();
+  cp_wait<0>();
+  __syncthreads();
+  build_t<FWD>(ys, Tg + tblock(s, bb, B0) * kTBuf, gsh + warp * kGBuf, warp, lane,
+               seg_off(g, 0) + 2 * t - g);
+}
 
-  // block transfers of 8 rows x 8 columns: lane -> (row r = lane/4, columns c0, c0+4)
-  const int io_r = lane >> 2, io_c = lane & 3;
-  const int io_colA = col0 + io_c, io_colB = col0 + io_c + 4;
-  const bool okA = io_colA < ncols, okB = io_colB < ncols;
-  double* colA = X + (long)(okA ? io_colA : 0) * ldX;
-  double* colB = X + (long)(okB ? io_colB : 0) * ldX;
+// One group (segment J) of the current block on the warp's window tiles
+// 4J .. 4J+4: W = X^T Y, W <- W (-T or -T^T), X^T += W Y^T.
+template <int J>
+__device__ __forceinline__ void apply_group(double (&x)[kTiles][4], const double* ys,
+                                            const double* ts, int lane, int offW, int offU0,
+                                            int offU1) {
+  double wa[4] = {0.0, 0.0, 0.0, 0.0}, wb[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int ti = 4 * J + i;
+    const double b0 = ys[offW + J * kSeg + 8 * i];
+    const double b1 = ys[offW + J * kSeg + 8 * i + 1];
+    if (i & 1)
+      mma16(wb, x[ti][0], x[ti][2], x[ti][1], x[ti][3], b0, b1);
+    else
+      mma16(wa, x[ti][0], x[ti][2], x[ti][1], x[ti][3], b0, b1);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) wa[q] += wb[q];
+  double wt[4] = {0.0, 0.0, 0.0, 0.0};
+  const double2 tf = *reinterpret_cast<const double2*>(ts + J * 64 + lane * 2);
+  mma16(wt, wa[0], wa[2], wa[1], wa[3], tf.x, tf.y);
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int ti = 4 * J + i;
+    const double b0 = ys[offU0 + J * kSeg + 8 * i];
+    const double b1 = ys[offU1 + J * kSeg + 8 * i];
+    mma16(x[ti], wt[0], wt[2], wt[1], wt[3], b0, b1);
+  }
+}
 
-  const int nstrips = (n - 2 + kWin - 1) / kWin;
+// First and second half of a block: segments 3,2 then 1,0 (forward) or 0,1
+// then 2,3 (reverse).
+template <bool FWD>
+__device__ __forceinline__ void apply_groups_lo(double (&x)[kTiles][4], const double* ys,
+                                                const double* ts, int lane, int offW, int offU0,
+                                                int offU1) {
+  apply_group<FWD ? 3 : 0>(x, ys, ts, lane, offW, offU0, offU1);
+  apply_group<FWD ? 2 : 1>(x, ys, ts, lane, offW, offU0, offU1);
+}
+template <bool FWD>
+__device__ __forceinline__ void apply_groups_hi(double (&x)[kTiles][4], const double* ys,
+                                                const double* ts, int lane, int offW, int offU0,
+                                                int offU1) {
+  apply_group<FWD ? 1 : 2>(x, ys, ts, lane, offW, offU0, offU1);
+  apply_group<FWD ? 0 : 3>(x, ys, ts, lane, offW, offU0, offU1);
+}
+
+// Window tile i of a frame starting at row `base`: rows base+8i .. base+8i+7.
+// Lane (g, t) holds X(rows 2t, 2t+1 of the tile; columns g, g+8 of the warp).
+struct TileIO {
+  double* cg;   // column c0+g (or a dummy)
+  double* cg8;  // column c0+g+8
+  bool okg, okg8;
+  int t2;
+};
+
+__device__ __forceinline__ void load_tile(double (&v)[4], const TileIO& io, long row0, int n) {
+  const long r = row0 + io.t2;
+  const bool r0 = r >= 0 && r < n, r1 = r + 1 >= 0 && r + 1 < n;
+  v[0] = (io.okg && r0) ? io.cg[r] : 0.0;
+  v[1] = (io.okg && r1) ? io.cg[r + 1] : 0.0;
+  v[2] = (io.okg8 && r0) ? io.cg8[r] : 0.0;
+  v[3] = (io.okg8 && r1) ? io.cg8[r + 1] : 0.0;
+}
+__device__ __forceinline__ void store_tile(const double (&v)[4], const TileIO& io, long row0,
+                                           int n) {
+  const long r = row0 + io.t2;
+  const bool r0 = r >= 0 && r < n, r1 = r + 1 >= 0 && r + 1 < n;
+  if (io.okg && r0) io.cg[r] = v[0];
+  if (io.okg && r1) io.cg[r + 1] = v[1];
+  if (io.okg8 && r0) io.cg8[r] = v[2];
+  if (io.okg8 && r1) io.cg8[r + 1] = v[3];
+}
+
+// PRE: the -T fragments were precomputed into Tg by q2_tbuild_kernel and are
+// staged with the reflectors; otherwise each block's T is built here, one
+// block ahead, by the same warps.
+template <bool FWD, bool PRE>
+__global__ void __launch_bounds__(kQThreads, 2)
+    q2_mma_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
+                  const double* __restrict__ Tg, double* __restrict__ X, long ldX) {
+  extern __shared__ __align__(16) double smem[];
+  double* Ys = smem;                 // kNYBuf x kYBuf
+  double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kTBuf (PRE) or 2 x kTBuf
+  double* Gs = Ts + kNYBuf * kTBuf;  // kQW x kGBuf
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  double* gs = Gs + warp * kGBuf;
+
+  // the zero padding of the staged segments is written once; staging never
+  // touches it
+  for (int e = threadIdx.x; e < kNYBuf * kYBuf; e += kQThreads) Ys[e] = 0.0;
+
+  // per-lane fragment offsets (segment 0 of the block)
+  const int offW = seg_off(g, 0) + 2 * t - g;               // Y[8i+2t(+1)][g]
+  const int offU0 = seg_off(2 * t, 0) + g - 2 * t;          // Y[8i+g][2t]
+  const int offU1 = seg_off(2 * t + 1, 0) + g - 2 * t - 1;  // Y[8i+g][2t+1]
+
+  const int c0 = blockIdx.x * (kQW * kQCols) + warp * kQCols;
+  TileIO io;
+  io.okg = c0 + g < ncols;
+  io.okg8 = c0 + g + 8 < ncols;
+  io.cg = X + (long)(io.okg ? c0 + g : 0) * ldX;
+  io.cg8 = X + (long)(io.okg8 ? c0 + g + 8 : 0) * ldX;
+  io.t2 = 2 * t;
+
+  double x[kTiles][4];
+  const int nstrips = (n - 2 + kStrip - 1) / kStrip;
+  const int B0 = (n - 2 + 7) / 8;
+  // stage the -T fragments of block bb of strip sidx (one 16-byte copy per thread)
+  auto stage_t = [&](double* dst, int sidx, int bb) {
+    const double* src = Tg + tblock(sidx, bb, B0) * kTBuf;
+    for (int e = threadIdx.x; e < kTBuf / 2; e += kQThreads) cp_async16(dst + 2 * e, src + 2 * e);
+  };
   for (int si = 0; si < nstrips; ++si) {
     const int sidx = FWD ? (nstrips - 1 - si) : si;
-    const long R = (long)sidx * kWin;
-    const int H = n - 2 - (int)R;            // sweeps with reflectors in this strip
-    if (H <= 0) continue;
-    const int nchunks = (H + kChunk - 1) / kChunk;
-    const int Hp = nchunks * kChunk;
+    const long R = (long)sidx * kStrip;
+    const int H = n - 2 - (int)R;  // sweeps with reflectors in this strip
+    const int nblk = (H + 7) / 8;
+    auto bb_of = [&](int it) { return FWD ? it : (nblk - 1 - it); };
 
-    // ---- load the initial window ----
-    // FWD: window of sweep 0 starts at row R+1.  REV: of sweep Hp-1 at R+Hp.
-    const long ws0 = FWD ? (R + 1) : (R + Hp);
-    double x[kCols][8];
-#pragma unroll
-    for (int c = 0; c < kCols; ++c) {
-      const int col = col0 + c;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        long row = ws0 + 8 * lane + j;
-        x[c][j] = (col < ncols && row < n) ? X[row + (long)col * ldX] : 0.0;
-      }
-    }
-    __syncthreads();
-    stage_chunk(Ubuf, U, ldU, n, R, H, FWD ? 0 : (nchunks - 1) * kChunk);
-    cp_commit();
-    // incoming rows for block 0: FWD rows R+257+r; REV rows R+Hp-1-r
+    __syncthreads();  // previous strip done with Ys / Ts; zero fill visible
     {
-      long row = FWD ? (R + 257 + io_r) : (R + Hp - 1 - io_r);
-      const bool rok = row < n && row >= 0;
-      inbuf[io_r * kCols + io_c] = (okA && rok) ? colA[row] : 0.0;
-      inbuf[io_r * kCols + io_c + 4] = (okB && rok) ? colB[row] : 0.0;
+      const long base = R + 8L * bb_of(0) + 1;
+#pragma unroll
+      for (int i = 0; i < kTiles; ++i) load_tile(x[i], io, base + 8 * i, n);
     }
-
-    for (int ck = 0; ck < nchunks; ++ck) {
-      const int chunk = FWD ? ck : (nchunks - 1 - ck);
-      const double* cur = Ubuf + (ck & 1) * (kChunk * kWin);
-      cp_wait_all();
-      __syncthreads();
-      if (ck + 1 < nchunks)
-        stage_chunk(Ubuf + ((ck + 1) & 1) * (kChunk * kWin), U, ldU, n, R, H,
-                    (FWD ? (chunk + 1) : (chunk - 1)) * kChunk);
-      cp_commit();
+    stage_block(Ys, U, ldU, n, R, H, bb_of(0));
+    if (PRE) stage_t(Ts, sidx, bb_of(0));
+    cp_commit();
+    if (nblk > 1) {
+      stage_block(Ys + kYBuf, U, ldU, n, R, H, bb_of(1));
+      if (PRE) stage_t(Ts + kTBuf, sidx, bb_of(1));
+    }
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();
+    if (!PRE) build_t<FWD>(Ys, Ts, gs, warp, lane, offW);
 
 #pragma unroll 1
-      for (int blk = 0; blk < kChunk / 8; ++blk) {
-        const int hb = FWD ? (chunk * kChunk + blk * 8) : (chunk * kChunk + kChunk - 1 - blk * 8);
-        const int gblk = ck * (kChunk / 8) + blk;
-        const double* in_cur = inbuf + (gblk & 1) * (8 * kCols);
-        double* in_nxt = inbuf + ((gblk + 1) & 1) * (8 * kCols);
-        // prefetch the next block's incoming rows
-        double preA, preB;
-        {
-          long row = FWD ? (R + hb + 8 + 257 + io_r) : (R + hb - 8 - io_r);
-          const bool rok = row < n && row >= 0;
-          preA = (okA && rok) ? colA[row] : 0.0;
-          preB = (okB && rok) ? colB[row] : 0.0;
-        }
+    for (int it = 0; it < nblk; ++it) {
+      const int bb = bb_of(it);
+      const long base = R + 8L * bb + 1;
+      cp_wait<0>();
+      __syncthreads();  // block it+1 staged; T of block it complete
+      if (it + 2 < nblk) {
+        stage_block(Ys + ((it + 2) % 3) * kYBuf, U, ldU, n, R, H, bb_of(it + 2));
+        if (PRE) stage_t(Ts + ((it + 2) % 3) * kTBuf, sidx, bb_of(it + 2));
+      }
+      cp_commit();
+      double inc[4];
+      load_tile(inc, io, FWD ? (base + 8 * kTiles) : (base - 8), n);
+      const double* ys = Ys + (it % 3) * kYBuf;
+      const double* ts = Ts + (PRE ? (it % 3) : (it & 1)) * kTBuf;
+      apply_groups_lo<FWD>(x, ys, ts, lane, offW, offU0, offU1);
+      if (!PRE && it + 1 < nblk)
+        build_t<FWD>(Ys + ((it + 1) % 3) * kYBuf, Ts + ((it + 1) & 1) * kTBuf, gs, warp, lane,
+                     offW);
+      apply_groups_hi<FWD>(x, ys, ts, lane, offW, offU0, offU1);
+      // slide the window one tile: the tile leaving it is final for this strip
+      if (FWD) {
+        store_tile(x[0], io, base, n);
 #pragma unroll
-        for (int P = 0; P < 8; ++P) {
-          const int h = FWD ? (hb + P) : (hb - P);
-          const double* us = cur + (h - chunk * kChunk) * kWin;
-          double u[8];
+        for (int i = 0; i + 1 < kTiles; ++i)
 #pragma unroll
-          for (int j = 0; j < 8; ++j) u[j] = us[uslot(lane, j)];
-          double d[kCols];
+          for (int q = 0; q < 4; ++q) x[i][q] = x[i + 1][q];
 #pragma unroll
-          for (int c = 0; c < kCols; ++c) {
-            double d0 = 0.0, d1 = 0.0;
+        for (int q = 0; q < 4; ++q) x[kTiles - 1][q] = inc[q];
+      } else {
+        store_tile(x[kTiles - 1], io, base + 8 * (kTiles - 1), n);
 #pragma unroll
-            for (int j = 0; j < 8; j += 2) {
-              d0 = fma(u[j], x[c][FWD ? ((j + P) & 7) : ((j - P) & 7)], d0);
-              d1 = fma(u[j + 1], x[c][FWD ? ((j + 1 + P) & 7) : ((j + 1 - P) & 7)], d1);
-            }
-            d[c] = d0 + d1;
-          }
+        for (int i = kTiles - 1; i > 0; --i)
 #pragma unroll
-          for (int c = 0; c < kCols; ++c) d[c] += __shfl_xor_sync(0xffffffffu, d[c], 1);
+          for (int q = 0; q < 4; ++q) x[i][q] = x[i - 1][q];
 #pragma unroll
-          for (int c = 0; c < kCols; ++c) d[c] += __shfl_xor_sync(0xffffffffu, d[c], 2);
-#pragma unroll
-          for (int c = 0; c < kCols; ++c)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              const int pj = FWD ? ((j + P) & 7) : ((j - P) & 7);
-              x[c][pj] = fma(-d[c], u[j], x[c][pj]);
-            }
-          // slide the window by one row (register ring, phase P is a constant):
-          // FWD: logical row 0 (physical P) leaves through lane 0 and every lane
-          //      takes lane l+1's; REV: logical row 7 (physical (7-P)&7) leaves
-          //      through lane 31 and every lane takes lane l-1's.  The rotation
-          //      hands the leaving value to the lane that receives the new row.
-          const int pp = FWD ? (P & 7) : ((7 - P) & 7);
-          const int src = FWD ? ((lane + 1) & 31) : ((lane + 31) & 31);
-          const bool edge = FWD ? (lane == 31) : (lane == 0);
-#pragma unroll
-          for (int c = 0; c < kCols; ++c) {
-            const double t = __shfl_sync(0xffffffffu, x[c][pp], src);
-            const double inv = in_cur[P * kCols + c];
-            if (edge) outbuf[P * kCols + c] = t;
-            x[c][pp] = edge ? inv : t;
-          }
-        }
-        __syncwarp();
-        // write back the 8 rows that left the window, stage the next incoming rows
-        {
-          long row = FWD ? (R + hb + 1 + io_r) : (R + hb + 256 - io_r);
-          if (row < n) {
-            if (okA) colA[row] = outbuf[io_r * kCols + io_c];
-            if (okB) colB[row] = outbuf[io_r * kCols + io_c + 4];
-          }
-          in_nxt[io_r * kCols + io_c] = preA;
-          in_nxt[io_r * kCols + io_c + 4] = preB;
-        }
-        __syncwarp();
+        for (int q = 0; q < 4; ++q) x[0][q] = inc[q];
       }
     }
-    // Every sweep is followed by a one-row slide and Hp % 8 == 0 (phase back
-    // to 0): FWD ends with the window at R+Hp+1, REV at R (one above sweep 0's).
-    const long wsf = FWD ? (R + Hp + 1) : R;
+    // the window now holds the frame one block past the last one
+    {
+      const long base = FWD ? (R + 8L * nblk + 1) : (R - 7);
 #pragma unroll
-    for (int c = 0; c < kCols; ++c) {
-      const int col = col0 + c;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        long row = wsf + 8 * lane + j;
-        if (col < ncols && row < n) X[row + (long)col * ldX] = x[c][j];
-      }
+      for (int i = 0; i < kTiles; ++i) store_tile(x[i], io, base + 8 * i, n);
     }
-    __syncthreads();
   }
 }
 
-constexpr size_t kBCSmem =
-    (2 * kChunk * kWin + kWarps * 3 * 8 * kCols) * sizeof(double);
-
-template <bool FWD>
-int launch_q2(long n, long ncols, const double* U, long ldU, double* X, long ldX,
-              cudaStream_t st) {
+template <bool FWD, bool PRE>
+int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
+              long ldX, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    EVD_CUDA_TRY(cudaFuncSetAttribute(q2_apply_kernel<FWD>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBCSmem));
+    EVD_CUDA_TRY(cudaFuncSetAttribute(q2_mma_kernel<FWD, PRE>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
     attr = true;
   }
-  int grid = ceil_div_i(ncols, kWarps * kCols);
-  q2_apply_kernel<FWD><<<grid, kThreadsBC, kBCSmem, st>>>((int)n, (int)ncols, U, ldU, X, ldX);
+  int grid = ceil_div_i((int)ncols, kQW * kQCols);
+  q2_mma_kernel<FWD, PRE><<<grid, kQThreads, kQSmem, st>>>((int)n, (int)ncols, U, ldU, Tg, X,
+                                                           ldX);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+template <bool FWD>
+int launch_tbuild(long n, const double* U, long ldU, double* Tg, cudaStream_t st) {
+  const int nstrips = (int)((n - 2 + kStrip - 1) / kStrip);
+  const int B0 = (int)((n - 2 + 7) / 8);
+  q2_tbuild_kernel<FWD><<<dim3(B0, nstrips), kQThreads, 0, st>>>((int)n, U, ldU, Tg);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
 }  // namespace
 
+long q2_tbuf_doubles(long n) {
+  if (n < 3) return 0;
+  const long nstrips = (n - 2 + kStrip - 1) / kStrip;
+  const long B0 = (n - 2 + 7) / 8;
+  return tblock(nstrips, 0, B0) * kTBuf;
+}
+
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
-             cudaStream_t st) {
+             double* tbuf, cudaStream_t st) {
   if (n < 0 || ncols < 0 || ldU < n || ldX < n) return EVD_ERR_INVALID_ARG;
   if (n > (1L << 30) || ncols > (1L << 30)) return EVD_ERR_INVALID_ARG;
   if (n < 3 || ncols == 0) return EVD_SUCCESS;
   if (!U || !X) return EVD_ERR_INVALID_ARG;
-  return forward ? launch_q2<true>(n, ncols, U, ldU, X, ldX, st)
-                 : launch_q2<false>(n, ncols, U, ldU, X, ldX, st);
+  if (tbuf && ((uintptr_t)tbuf & 15)) return EVD_ERR_INVALID_ARG;
+  if (tbuf) {
+    if (forward) {
+      EVD_TRY(launch_tbuild<true>(n, U, ldU, tbuf, st));
+      return launch_q2<true, true>(n, ncols, U, ldU, tbuf, X, ldX, st);
+    }
+    EVD_TRY(launch_tbuild<false>(n, U, ldU, tbuf, st));
+    return launch_q2<false, true>(n, ncols, U, ldU, tbuf, X, ldX, st);
+  }
+  return forward ? launch_q2<true, false>(n, ncols, U, ldU, nullptr, X, ldX, st)
+                 : launch_q2<false, false>(n, ncols, U, ldU, nullptr, X, ldX, st);
 }
 
 }  // namespace evd
 
+extern "C" long evd_bc_back_work_size(long n) { return evd::q2_tbuf_doubles(n < 0 ? 0 : n); }
+
 extern "C" int evd_bc_back(double* Q, long ldQ, const double* U, long ldU, long n, int b,
                            cudaStream_t stream) {
   if (b != 32) return EVD_ERR_INVALID_ARG;
-  return evd::q2_apply(true, n, n, U, ldU, Q, ldQ, stream);
+  return evd::q2_apply(true, n, n, U, ldU, Q, ldQ, nullptr, stream);
 }
 
 extern "C" int evd_bc_back_apply(long n, long ncols, const double* U, long ldU, double* X,
-                                 long ldX, int b, cudaStream_t stream) {
+                                 long ldX, int b, double* work, long lwork, cudaStream_t stream) {
   if (b != 32) return EVD_ERR_INVALID_ARG;
-  return evd::q2_apply(false, n, ncols, U, ldU, X, ldX, stream);
+  if (work && lwork < evd::q2_tbuf_doubles(n)) return EVD_ERR_WORKSPACE;
+  return evd::q2_apply(false, n, ncols, U, ldU, X, ldX, work, stream);
 }

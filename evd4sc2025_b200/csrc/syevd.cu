@@ -35,8 +35,9 @@ long stedc_ws_doubles(long n);
 long stedc_ws_ints(long n);
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
           long liwork, cudaStream_t st);
+long q2_tbuf_doubles(long n);
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
-             cudaStream_t st);
+             double* tbuf, cudaStream_t st);
 long sbr_back_ws_doubles(long n, long b, long nk);
 int wy_merge_slabs(long n, long b, long nk, long ncolsWY, double* dW, long ldW, const double* dY,
                    long ldY, double* work, cudaStream_t st);
@@ -123,7 +124,10 @@ int syevd(long n, long b, long nb, const double* A, long lda, double* w, double*
   EVD_TRY(stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[3], st));
   // ---- back transformations ----
-  EVD_TRY(q2_apply(false, n, n, U, n, X, ldX, st));
+  // the T factors of the chasing reflectors go into OA (free after stage 1);
+  // for very small n they do not fit and the kernel rebuilds them itself
+  double* tbuf = ((size_t)q2_tbuf_doubles(n) <= (size_t)n * n) ? OA : nullptr;
+  EVD_TRY(q2_apply(false, n, n, U, n, X, ldX, tbuf, st));
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[4], st));
   const long npcols = ((n - 1) / b) * b;
   EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, st));

@@ -169,9 +169,14 @@ int evd_bc_back(double* Q, long ldQ, const double* U, long ldU, long n, int b,
                 cudaStream_t stream);
 
 /* X <- Q2 * X for an n x ncols block X (the eigenvector direction: reflectors
- * applied in reverse generation order). */
+ * applied in reverse generation order; the reference applies Q2 through
+ * my_SBRBack_BCBack, src/EVD/myEVD.cu:135-249).  `work` (16-byte aligned,
+ * evd_bc_back_work_size(n) doubles, about n^2/8) receives the compact-WY
+ * T factors of the reflector groups, built once for all columns; with
+ * work == NULL they are rebuilt inside the apply kernel (slower). */
+long evd_bc_back_work_size(long n);
 int evd_bc_back_apply(long n, long ncols, const double* U, long ldU, double* X, long ldX,
-                      int b, cudaStream_t stream);
+                      int b, double* work, long lwork, cudaStream_t stream);
 
 /* Merge the b-wide compact-WY slides of an M x N block into one compact WY:
  * W[:, i-b:i] -= W[:, 0:i-b] * (Y[:, 0:i-b]^T * W[:, i-b:i]) for i = 2b..N.

@@ -34,6 +34,36 @@ def test_q2_apply_matches_oracle(cuda, evdlib, n, ncols, forward):
     assert np.abs(Xd.cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.sqrt(n))
 
 
+@pytest.mark.parametrize("n,ncols", [(5, 3), (257, 64), (517, 133), (1100, 300)])
+def test_q2_apply_without_workspace(cuda, evdlib, n, ncols):
+    """X <- Q2 X with the T factors rebuilt inside the kernel (work = NULL)
+    agrees with the precomputed-T path and with the oracle."""
+    U = _chase_U(n, seed=n + 1)
+    X = np.random.default_rng(ncols).standard_normal((n, ncols))
+    ref = O.q2_apply(X, U, n, 32, transpose=False)
+    Ud = evdlib.to_cm(torch.from_numpy(U), device=cuda)
+    X1 = evdlib.to_cm(torch.from_numpy(X), device=cuda)
+    X2 = evdlib.to_cm(torch.from_numpy(X), device=cuda)
+    evdlib.bc_back_apply(X1, Ud, work=None)
+    evdlib.bc_back_apply(X2, Ud, work=True)
+    torch.cuda.synchronize()
+    a, b = X1.cpu().numpy(), X2.cpu().numpy()
+    assert np.abs(a - ref).max() <= 1e-12 * max(1.0, np.sqrt(n))
+    assert np.abs(a - b).max() <= 1e-13 * max(1.0, np.sqrt(n))
+
+
+def test_q2_apply_rejects_small_workspace(cuda, evdlib):
+    import ctypes as C
+    n = 300
+    U = evdlib.zeros_cm(n, n, device=cuda)
+    X = evdlib.zeros_cm(n, 4, device=cuda)
+    need = evdlib.lib().evd_bc_back_work_size(n)
+    w = torch.empty(need, dtype=torch.float64, device=cuda)
+    rc = evdlib.lib().evd_bc_back_apply(n, 4, C.c_void_p(U.data_ptr()), n, C.c_void_p(X.data_ptr()),
+                                        n, 32, C.c_void_p(w.data_ptr()), need - 1, None)
+    assert rc == -5  # EVD_ERR_WORKSPACE
+
+
 def _fwd(evdlib, Xd, Ud):
     """Q2^T X for any column count through the square reference entry point:
     process X in chunks of at most n columns padded into an n x n block."""
