@@ -329,6 +329,247 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
       }
 }
 
+// ---------------------------------------------------------------------------
+// Lean variant of dgemm_kernel for the common cases (no M-split operand pair,
+// 16-byte aligned operands, K-split pair only at a multiple of BK): every
+// thread's share of a tile copy is fixed at kernel start (one contiguous
+// offset, one strided line plus a fixed stride per pass), so a k-tile costs
+// one pointer computation per operand and a predicate per chunk instead of a
+// full address computation per chunk.  Plain products use grouped
+// rasterisation (kRaster tile rows at a time) so that the CTAs resident at
+// once share their A and B panels in L2.
+constexpr int kRaster = 8;
+
+// Per-thread copy of a (CL contiguous x SL strided) tile into smem laid out
+// [strided][CL + kPad], in 16-byte chunks.
+template <int CL, int SL, int NT>
+struct TileCopy {
+  static constexpr int CH = CL / 2;  // chunks per strided line
+  static_assert(NT % CH == 0, "threads must cover whole lines");
+  static constexpr int SS = NT / CH;  // lines per pass
+  static_assert(SL % SS == 0, "passes must cover the tile");
+  static constexpr int R = SL / SS;   // passes
+  static_assert(R <= 32, "predicate mask");
+  int ci, si0;
+  __device__ __forceinline__ void init() {
+    ci = (threadIdx.x % CH) * 2;
+    si0 = threadIdx.x / CH;
+  }
+  // bytes valid from contiguous index c (relative) given `rem` valid elements
+  __device__ __forceinline__ static int cbytes(int rem) { return rem >= 2 ? 16 : (rem == 1 ? 8 : 0); }
+  // strided lines si0 + r*SS < lim
+  __device__ __forceinline__ unsigned smask(int lim) const {
+    unsigned mk = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (si0 + r * SS < lim) mk |= 1u << r;
+    return mk;
+  }
+  __device__ __forceinline__ void issue(double* smem, const double* g, long step, int cb,
+                                        unsigned mk, const double* safe) const {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int bytes = ((mk >> r) & 1u) ? cb : 0;
+      cp_async16(smem + (si0 + r * SS) * (CL + kPad) + ci, bytes ? g + (long)r * step : safe,
+                 bytes);
+    }
+  }
+};
+
+template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA>
+__global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
+    dgemm_fast_kernel(const GemmArgs p) {
+  constexpr int NWM = BM / WM, NWN = BN / WN;
+  constexpr int NT = NWM * NWN * 32;
+  constexpr int MR = (MMA >= 1) ? 16 : 8;
+  constexpr int NC = (MMA >= 1) ? 4 : 2;
+  constexpr int KS = (MMA == 3) ? 16 : ((MMA == 2) ? 8 : 4);
+  constexpr int NA = (MMA == 3) ? 8 : ((MMA == 2) ? 4 : ((MMA == 1) ? 2 : 1));
+  constexpr int NB = KS / 4;
+  constexpr int MI = WM / MR, NJ = WN / 8;
+  using AT = ATile<TA, BM, BK>;
+  using BT = BTile<TB, BN, BK>;
+  using ACopy = TileCopy<TA ? BK : BM, TA ? BM : BK, NT>;
+  using BCopy = TileCopy<TB ? BN : BK, TB ? BK : BN, NT>;
+
+  extern __shared__ __align__(16) double smem[];
+  double* As = smem;
+  double* Bs = smem + STAGES * AT::kSize;
+
+  int tm, tn, z = blockIdx.y;
+  if (p.mode == kSyr2kLow) {
+    int T = p.tiles_m;
+    long bid = blockIdx.x;
+    double Td = T + 0.5;
+    int tj = (int)(Td - sqrt(Td * Td - 2.0 * (double)bid));
+    if (tj < 0) tj = 0;
+    if (tj > T - 1) tj = T - 1;
+    while (tj > 0 && (long)tj * T - (long)tj * (tj - 1) / 2 > bid) --tj;
+    while ((long)(tj + 1) * T - (long)(tj + 1) * tj / 2 <= bid) ++tj;
+    long start = (long)tj * T - (long)tj * (tj - 1) / 2;
+    tn = tj;
+    tm = tj + (int)(bid - start);
+  } else {
+    // grouped rasterisation: kRaster tile rows, column by column
+    const int id = blockIdx.x;
+    const int span = kRaster * p.tiles_n;
+    const int grp = id / span, first = grp * kRaster;
+    const int gm = min(kRaster, p.tiles_m - first);
+    const int in = id - grp * span;
+    tm = first + in % gm;
+    tn = in / gm;
+  }
+  const int m0 = tm * BM, n0 = tn * BN;
+
+  int batch = z, split = 0;
+  if (p.splitk > 1) {
+    batch = z / p.splitk;
+    split = z % p.splitk;
+  }
+  const double* Ab = p.A + (long)batch * p.sA;
+  const double* Bb = p.B + (long)batch * p.sB;
+
+  const int ktot = p.k;
+  int kbeg = 0, kend = ktot;
+  if (p.splitk > 1) {
+    int ktiles = (ktot + BK - 1) / BK;
+    int per = (ktiles + p.splitk - 1) / p.splitk;
+    kbeg = min(ktot, split * per * BK);
+    kend = min(ktot, (split + 1) * per * BK);
+  }
+  const int KT = (kend - kbeg + BK - 1) / BK;
+
+  ACopy ac;
+  BCopy bc;
+  ac.init();
+  bc.init();
+  // fixed predicates along M / N
+  int a_cb = 16, b_cb = 16;
+  unsigned a_mk = ~0u, b_mk = ~0u;
+  if (!TA) a_cb = ACopy::cbytes(p.m - m0 - ac.ci);
+  else a_mk = ac.smask(p.m - m0);
+  if (TB) b_cb = BCopy::cbytes(p.n - n0 - bc.ci);
+  else b_mk = bc.smask(p.n - n0);
+
+  auto issue = [&](int kt, int stage) {
+    const int k0 = kbeg + kt * BK;
+    const int klim = kend - k0;  // valid K in this tile (may exceed BK)
+    double* as = As + stage * AT::kSize;
+    double* bs = Bs + stage * BT::kSize;
+    if (!TA) {
+      const bool second = k0 >= p.k1;
+      const double* base = second ? p.A2 : Ab;
+      const long ld = second ? p.lda2 : p.lda;
+      const int kk = second ? k0 - p.k1 : k0;
+      const double* g = base + (long)(m0 + ac.ci) + (long)(kk + ac.si0) * ld;
+      const unsigned mk = (klim >= BK) ? ~0u : ac.smask(klim);
+      ac.issue(as, g, (long)ACopy::SS * ld, a_cb, mk, p.A);
+    } else {
+      const double* g = Ab + (long)(k0 + ac.ci) + (long)(m0 + ac.si0) * p.lda;
+      const int cb = (klim >= BK) ? 16 : ACopy::cbytes(klim - ac.ci);
+      ac.issue(as, g, (long)ACopy::SS * p.lda, cb, a_mk, p.A);
+    }
+    if (!TB) {
+      const double* g = Bb + (long)(k0 + bc.ci) + (long)(n0 + bc.si0) * p.ldb;
+      const int cb = (klim >= BK) ? 16 : BCopy::cbytes(klim - bc.ci);
+      bc.issue(bs, g, (long)BCopy::SS * p.ldb, cb, b_mk, p.B);
+    } else {
+      const bool second = k0 >= p.k1;
+      const double* base = second ? p.B2 : Bb;
+      const long ld = second ? p.ldb2 : p.ldb;
+      const int kk = second ? k0 - p.k1 : k0;
+      const double* g = base + (long)(n0 + bc.ci) + (long)(kk + bc.si0) * ld;
+      const unsigned mk = (klim >= BK) ? ~0u : bc.smask(klim);
+      bc.issue(bs, g, (long)BCopy::SS * ld, b_cb, mk, p.B);
+    }
+  };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wm0 = (warp % NWM) * WM, wn0 = (warp / NWM) * WN;
+  const int g = lane >> 2, t = lane & 3;
+
+  double acc[MI][NJ][NC];
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int h = 0; h < NC; ++h) acc[i][j][h] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; ++s) {
+    if (s < KT) issue(s, s);
+    cp_async_commit();
+  }
+
+  for (int kt = 0; kt < KT; ++kt) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      int nk = kt + STAGES - 1;
+      if (nk < KT) issue(nk, nk % STAGES);
+      cp_async_commit();
+    }
+    const double* as = As + (kt % STAGES) * AT::kSize;
+    const double* bs = Bs + (kt % STAGES) * BT::kSize;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += KS) {
+      double a[MI][8], b[NJ][4];
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int q = 0; q < NA; ++q)
+          a[i][q] = as[AT::at(wm0 + i * MR + g + 8 * (q & 1), kk + t + 4 * (q >> 1))];
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int q = 0; q < NB; ++q) b[j][q] = bs[BT::at(kk + t + 4 * q, wn0 + j * 8 + g)];
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          double(&dd)[4] = *reinterpret_cast<double(*)[4]>(&acc[i][j][0]);
+          if (MMA == 3) dmma_16x8x16(dd, a[i], b[j]);
+          else if (MMA == 2) dmma_16x8x8(dd, a[i], b[j]);
+          else if (MMA == 1) dmma_16x8x4(dd, a[i][0], a[i][1], b[j][0]);
+          else dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i][0], b[j][0]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+
+  if (p.splitk > 1) {
+    double* W = p.ws + ((long)batch * p.splitk + split) * (long)p.m * p.n;
+#pragma unroll
+    for (int i = 0; i < MI; ++i)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j)
+#pragma unroll
+        for (int h = 0; h < NC; ++h) {
+          int r = m0 + wm0 + i * MR + g + 8 * (h >> 1), c = n0 + wn0 + j * 8 + 2 * t + (h & 1);
+          if (r < p.m && c < p.n) W[r + (long)c * p.m] = acc[i][j][h];
+        }
+    return;
+  }
+  double* Cb = p.C + (long)batch * p.sC;
+  const bool mirror = (p.mode == kSyr2kLow);
+#pragma unroll
+  for (int i = 0; i < MI; ++i)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int h = 0; h < NC; ++h) {
+        int r = m0 + wm0 + i * MR + g + 8 * (h >> 1), c = n0 + wn0 + j * 8 + 2 * t + (h & 1);
+        if (r >= p.m || c >= p.n) continue;
+        if (mirror && r < c) continue;
+        double* dst = Cb + r + (long)c * p.ldc;
+        double v = p.alpha * acc[i][j][h];
+        if (p.beta != 0.0) v = fma(p.beta, *dst, v);
+        *dst = v;
+        if (mirror && r != c) Cb[c + (long)r * p.ldc] = v;
+      }
+}
+
 __global__ void dgemm_splitk_reduce_kernel(int m, int n, int splits, long batch_count,
                                            const double* ws, double alpha, double beta,
                                            double* C, long ldc, long sC) {
@@ -349,12 +590,14 @@ __global__ void dgemm_splitk_reduce_kernel(int m, int n, int splits, long batch_
   }
 }
 
-template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA = 0>
+template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA = 0,
+          bool FAST = false>
 int launch_cfg(GemmArgs p, int grid_x, int grid_y, cudaStream_t st) {
   constexpr int NT = (BM / WM) * (BN / WN) * 32;
   constexpr size_t smem =
       STAGES * (ATile<TA, BM, BK>::kSize + BTile<TB, BN, BK>::kSize) * sizeof(double);
-  auto kern = dgemm_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>;
+  auto kern = FAST ? dgemm_fast_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>
+                   : dgemm_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>;
   static bool attr_set = false;  // per instantiation; set once per process
   if (!attr_set) {
     EVD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -375,13 +618,19 @@ int dispatch_shape(GemmArgs p, long batch, cudaStream_t st) {
   // Tile shapes chosen by measurement on B200 (DGEMM 8192^3: 64x64 tiles with
   // four 32x32 warps and m16n8k16 DMMA reach 30 TFLOP/s, 128x128 tiles 27;
   // the skinny n = 32 ZY products run best as 64x32 tiles with split-K).
+  // The lean kernel serves every call whose operands are 16-byte aligned and
+  // whose K-split operand pair (if any) switches at a multiple of BK = 16;
+  // the general kernel covers the rest (M-split pairs, odd alignments).
+  const bool fast = p.vecA && p.vecB && (p.Am2 == nullptr || p.m1 >= p.m) &&
+                    (p.k1 >= p.k || p.k1 % 16 == 0);
   if (p.n <= 32 && p.mode == kGemm) {
     constexpr int BM = 64, BN = 32;
     p.tiles_m = ceil_div_i(p.m, BM);
     p.tiles_n = ceil_div_i(p.n, BN);
     int grid_x = p.tiles_m * p.tiles_n;
     int grid_y = (int)batch * max(1, p.splitk);
-    return launch_cfg<TA, TB, BM, BN, 16, 16, 32, 4, 3>(p, grid_x, grid_y, st);
+    return fast ? launch_cfg<TA, TB, BM, BN, 16, 16, 32, 4, 3, true>(p, grid_x, grid_y, st)
+                : launch_cfg<TA, TB, BM, BN, 16, 16, 32, 4, 3>(p, grid_x, grid_y, st);
   }
   constexpr int BM = 64, BN = 64;
   p.tiles_m = ceil_div_i(p.m, BM);
@@ -389,7 +638,8 @@ int dispatch_shape(GemmArgs p, long batch, cudaStream_t st) {
   int grid_x = (p.mode == kSyr2kLow) ? p.tiles_m * (p.tiles_m + 1) / 2
                                      : p.tiles_m * p.tiles_n;
   int grid_y = (int)batch * max(1, p.splitk);
-  return launch_cfg<TA, TB, BM, BN, 16, 32, 32, 4, 3>(p, grid_x, grid_y, st);
+  return fast ? launch_cfg<TA, TB, BM, BN, 16, 32, 32, 4, 3, true>(p, grid_x, grid_y, st)
+              : launch_cfg<TA, TB, BM, BN, 16, 32, 32, 4, 3>(p, grid_x, grid_y, st);
 }
 
 }  // namespace
