@@ -297,110 +297,166 @@ __global__ void merge_setup_kernel(LevelArgs a) {
   a.zs[lo + rank] = zc;
 }
 
-// Sequential deflation, one thread per merge.  grid nm, block 32 (lane 0 works).
-__global__ void merge_deflate_kernel(LevelArgs a) {
+// Deflation of one merge (LAPACK dlaed2's tests, the reference's host dstedc):
+// small components of z, then Givens pair deflation of neighbours in the merged
+// order.  The pair test chains through the previous undeflated entry, so one
+// thread scans; the block stages the inputs in shared memory chunk by chunk
+// (the scan never waits on global loads), reduces the tolerance in parallel and
+// finishes the type-ordered GEMM positions in parallel.  grid nm, block
+// kDefThreads.
+constexpr int kDefThreads = 256;
+constexpr int kDefChunk = 2048;
+
+__global__ void __launch_bounds__(kDefThreads) merge_deflate_kernel(LevelArgs a) {
+  __shared__ double s_d[kDefChunk], s_z[kDefChunk];
+  __shared__ int s_c[kDefChunk];
+  __shared__ double s_red[2][kDefThreads / 32];
+  __shared__ int s_bad, s_K, s_K1, s_K2;
   const int m = blockIdx.x;
-  if (threadIdx.x != 0) return;
   const long lo = (long)m * a.N;
   const int N = a.N, n1 = a.n1;
   const double rho = a.rho[m];
   const double* ds = a.ds + lo;
   const double* zs = a.zs + lo;
   const int* perm = a.perm + lo;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   double dmax = 0.0, zmax = 0.0;
-  for (int k = 0; k < N; ++k) {
+  for (int k = tid; k < N; k += kDefThreads) {
     dmax = fmax(dmax, fabs(ds[k]));
     zmax = fmax(zmax, fabs(zs[k]));
   }
+  dmax = warp_max(dmax);
+  zmax = warp_max(zmax);
+  if (lane == 0) {
+    s_red[0][wid] = dmax;
+    s_red[1][wid] = zmax;
+  }
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  dmax = 0.0;
+  zmax = 0.0;
+  for (int w = 0; w < kDefThreads / 32; ++w) {
+    dmax = fmax(dmax, s_red[0][w]);
+    zmax = fmax(zmax, s_red[1][w]);
+  }
   const double tol = 8.0 * kEps * fmax(dmax, zmax);
-  int K = 0, nd = 0, nr = 0;
   int* d_ = a.desc + 8 * m;
   if (rho * zmax <= tol) {
-    for (int k = 0; k < N; ++k) {
-      a.dD[lo + nd] = ds[k];
-      a.colD[lo + nd] = perm[k];
-      ++nd;
+    // everything deflates: the merged order is the result
+    for (int k = tid; k < N; k += kDefThreads) {
+      a.dD[lo + k] = ds[k];
+      a.colD[lo + k] = perm[k];
     }
-  } else {
-    bool have = false;
-    double pd = 0.0, pz = 0.0;
-    int pc = 0, pt = 0;
-    for (int k = 0; k < N; ++k) {
-      double dk = ds[k], zk = zs[k];
-      int ck = perm[k];
-      if (ck < 0 || ck >= N) {
-        atomicCAS(a.err, 0, kDevBadShape);
-        return;
-      }
-      int tk = (ck < n1) ? 1 : 3;
-      if (rho * fabs(zk) <= tol) {
-        a.dD[lo + nd] = dk;
-        a.colD[lo + nd] = ck;
-        ++nd;
-        continue;
-      }
-      if (!have) {
-        have = true;
-        pd = dk; pz = zk; pc = ck; pt = tk;
-        continue;
-      }
-      double sv = pz, cv = zk;
-      double tau = hypot(cv, sv);
-      double t = dk - pd;
-      cv /= tau;
-      sv = -sv / tau;
-      if (fabs(t * cv * sv) <= tol) {
-        // rotate columns (pc, ck): x' = c x + s y, y' = c y - s x
-        a.rA[lo + nr] = pc;
-        a.rB[lo + nr] = ck;
-        a.rc[lo + nr] = cv;
-        a.rs[lo + nr] = sv;
-        ++nr;
-        double c2 = cv * cv, s2 = sv * sv;
-        double dnew_p = pd * c2 + dk * s2;
-        double dnew_k = pd * s2 + dk * c2;
-        int tnew = (pt == tk) ? tk : 2;
-        // previous deflates
-        a.dD[lo + nd] = dnew_p;
-        a.colD[lo + nd] = pc;
-        ++nd;
-        pd = dnew_k; pz = tau; pc = ck; pt = tnew;
-      } else {
-        a.dK[lo + K] = pd;
-        a.zK[lo + K] = pz;
-        a.colK[lo + K] = pc;
-        a.typK[lo + K] = pt;
-        ++K;
-        pd = dk; pz = zk; pc = ck; pt = tk;
-      }
+    if (tid == 0) {
+      d_[D_K] = 0;
+      d_[D_K1] = 0;
+      d_[D_K2] = 0;
+      d_[D_K3] = 0;
+      d_[D_NDEF] = N;
+      d_[D_NROT] = 0;
     }
-    if (have) {
-      a.dK[lo + K] = pd;
-      a.zK[lo + K] = pz;
-      a.colK[lo + K] = pc;
-      a.typK[lo + K] = pt;
-      ++K;
+    return;
+  }
+  // scan state (thread 0 only)
+  int K = 0, nd = 0, nr = 0, c1 = 0, c2 = 0, c3 = 0;
+  bool have = false;
+  double pd = 0.0, pz = 0.0;
+  int pc = 0, pt = 0;
+  auto emit_root = [&](double dv, double zv, int cv, int tv) {
+    a.dK[lo + K] = dv;
+    a.zK[lo + K] = zv;
+    a.colK[lo + K] = cv;
+    a.typK[lo + K] = tv;
+    a.pT[lo + K] = (tv == 1) ? c1++ : ((tv == 2) ? c2++ : c3++);  // index within its type
+    ++K;
+  };
+  for (int c0 = 0; c0 < N; c0 += kDefChunk) {
+    const int cn = min(kDefChunk, N - c0);
+    __syncthreads();  // previous chunk consumed
+    for (int k = tid; k < cn; k += kDefThreads) {
+      s_d[k] = ds[c0 + k];
+      s_z[k] = zs[c0 + k];
+      s_c[k] = perm[c0 + k];
+    }
+    __syncthreads();
+    if (tid == 0 && !s_bad) {
+      for (int k = 0; k < cn; ++k) {
+        const double dk = s_d[k], zk = s_z[k];
+        const int ck = s_c[k];
+        if (ck < 0 || ck >= N) {
+          atomicCAS(a.err, 0, kDevBadShape);
+          s_bad = 1;
+          break;
+        }
+        const int tk = (ck < n1) ? 1 : 3;
+        if (rho * fabs(zk) <= tol) {
+          a.dD[lo + nd] = dk;
+          a.colD[lo + nd] = ck;
+          ++nd;
+          continue;
+        }
+        if (!have) {
+          have = true;
+          pd = dk; pz = zk; pc = ck; pt = tk;
+          continue;
+        }
+        double sv = pz, cv = zk;
+        const double tau = hypot(cv, sv);
+        const double t = dk - pd;
+        cv /= tau;
+        sv = -sv / tau;
+        if (fabs(t * cv * sv) <= tol) {
+          // rotate columns (pc, ck): x' = c x + s y, y' = c y - s x
+          a.rA[lo + nr] = pc;
+          a.rB[lo + nr] = ck;
+          a.rc[lo + nr] = cv;
+          a.rs[lo + nr] = sv;
+          ++nr;
+          const double cc = cv * cv, ss = sv * sv;
+          const double dnew_p = pd * cc + dk * ss;
+          const double dnew_k = pd * ss + dk * cc;
+          const int tnew = (pt == tk) ? tk : 2;
+          a.dD[lo + nd] = dnew_p;  // the previous entry deflates
+          a.colD[lo + nd] = pc;
+          ++nd;
+          pd = dnew_k; pz = tau; pc = ck; pt = tnew;
+        } else {
+          emit_root(pd, pz, pc, pt);
+          pd = dk; pz = zk; pc = ck; pt = tk;
+        }
+      }
     }
   }
-  // type-ordered positions for the two structured GEMMs
-  int K1 = 0, K2 = 0, K3 = 0;
-  for (int i = 0; i < K; ++i) {
-    int t = a.typK[lo + i];
-    if (t == 1) ++K1; else if (t == 2) ++K2; else ++K3;
+  if (tid == 0) {
+    if (have && !s_bad) emit_root(pd, pz, pc, pt);
+    s_K = K;
+    s_K1 = c1;
+    s_K2 = c2;
+    d_[D_K] = K;
+    d_[D_K1] = c1;
+    d_[D_K2] = c2;
+    d_[D_K3] = c3;
+    d_[D_NDEF] = nd;
+    d_[D_NROT] = nr;
   }
-  int c1 = 0, c2 = 0, c3 = 0;
-  for (int i = 0; i < K; ++i) {
-    int t = a.typK[lo + i];
-    if (t == 1) { a.pT[lo + i] = c1++; a.pB[lo + i] = -1; }
-    else if (t == 2) { a.pT[lo + i] = K1 + c2; a.pB[lo + i] = c2; ++c2; }
-    else { a.pT[lo + i] = -1; a.pB[lo + i] = K2 + c3++; }
+  __syncthreads();
+  if (s_bad) return;
+  // type-ordered positions for the two structured GEMMs:
+  // type 1 -> Qt column c1; type 2 -> Qt column K1 + c2 and Qb column c2;
+  // type 3 -> Qb column K2 + c3
+  const int Kf = s_K, K1f = s_K1, K2f = s_K2;
+  for (int i = tid; i < Kf; i += kDefThreads) {
+    const int tv = a.typK[lo + i], idx = a.pT[lo + i];
+    if (tv == 1) {
+      a.pB[lo + i] = -1;
+    } else if (tv == 2) {
+      a.pT[lo + i] = K1f + idx;
+      a.pB[lo + i] = idx;
+    } else {
+      a.pT[lo + i] = -1;
+      a.pB[lo + i] = K2f + idx;
+    }
   }
-  d_[D_K] = K;
-  d_[D_K1] = K1;
-  d_[D_K2] = K2;
-  d_[D_K3] = K3;
-  d_[D_NDEF] = nd;
-  d_[D_NROT] = nr;
 }
 
 // Apply the recorded rotations to the block's columns; thread = row.
@@ -425,12 +481,15 @@ __global__ void merge_rotate_kernel(LevelArgs a) {
 }
 
 // Gather Q1/mixed columns (top rows) and mixed/Q2 columns (bottom rows) into
-// zero-padded Qt (n1 x K12max) and Qb (n2 x K23max); copy deflated columns to
-// Zn[:, K + t].  grid (ceil(N/256), nm), thread = row; loops over columns.
+// zero-padded Qt (n1 x K12max) and Qb (n2 x K23max).  grid (ceil(N/256),
+// ceil(Kcols/kColChunk), nm): thread = row, blockIdx.y = a chunk of columns.
+constexpr int kColChunk = 64;
+
 __global__ void merge_gather_kernel(LevelArgs a) {
-  const int m = blockIdx.y;
+  const int m = blockIdx.z;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.N) return;
+  const int j0 = blockIdx.y * kColChunk;
   const long lo = (long)m * a.N;
   const int* d_ = a.desc + 8 * m;
   const int K = d_[D_K], K1 = d_[D_K1], K2 = d_[D_K2], K3 = d_[D_K3];
@@ -438,11 +497,14 @@ __global__ void merge_gather_kernel(LevelArgs a) {
   double* Qt = a.Qt + (long)m * a.n1 * a.K12max;
   double* Qb = a.Qb + (long)m * a.n2 * a.K23max;
   if (r < a.n1) {
-    for (int j = K1 + K2; j < a.K12max; ++j) Qt[r + (long)j * a.n1] = 0.0;
+    for (int j = max(j0, K1 + K2); j < min(a.K12max, j0 + kColChunk); ++j)
+      Qt[r + (long)j * a.n1] = 0.0;
   } else {
-    for (int j = K2 + K3; j < a.K23max; ++j) Qb[(r - a.n1) + (long)j * a.n2] = 0.0;
+    for (int j = max(j0, K2 + K3); j < min(a.K23max, j0 + kColChunk); ++j)
+      Qb[(r - a.n1) + (long)j * a.n2] = 0.0;
   }
-  for (int i = 0; i < K; ++i) {
+  const int i1 = min(K, j0 + kColChunk);
+  for (int i = j0; i < i1; ++i) {
     long col = a.colK[lo + i];
     if (col < 0 || col >= a.N) {
       atomicCAS(a.err, 0, kDevBadShape);
@@ -461,10 +523,12 @@ __global__ void merge_gather_kernel(LevelArgs a) {
 
 // Deflated columns (after the rotations) -> Zn[:, K + t].  Runs after the
 // merge GEMMs, which write Zn[:, 0:Kmax] for every merge of the level.
+// grid (ceil(N/256), ceil(N/kColChunk), nm).
 __global__ void merge_copy_deflated_kernel(LevelArgs a) {
-  const int m = blockIdx.y;
+  const int m = blockIdx.z;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.N) return;
+  const int t0 = blockIdx.y * kColChunk;
   const long lo = (long)m * a.N;
   const int* d_ = a.desc + 8 * m;
   const int K = d_[D_K], nd = d_[D_NDEF];
@@ -474,7 +538,8 @@ __global__ void merge_copy_deflated_kernel(LevelArgs a) {
     atomicCAS(a.err, 0, kDevBadShape);
     return;
   }
-  for (int t = 0; t < nd; ++t) {
+  const int t1 = min(nd, t0 + kColChunk);
+  for (int t = t0; t < t1; ++t) {
     long col = a.colD[lo + t];
     if (col < 0 || col >= a.N) {
       atomicCAS(a.err, 0, kDevBadShape);
@@ -723,14 +788,19 @@ __global__ void merge_finalize_rank_kernel(LevelArgs a) {
   a.perm[lo + rank] = q;        // source column in Zn
 }
 
-// Zw[lo:hi, lo + p] = Zn[:, perm[p]], dw[lo + p] = sorted value.  thread = row.
+// Zw[lo:hi, lo + p] = Zn[:, perm[p]], dw[lo + p] = sorted value.
+// grid (ceil(N/256), ceil(N/kColChunk), nm): thread = row, blockIdx.y = columns.
 __global__ void merge_scatter_kernel(LevelArgs a) {
-  const int m = blockIdx.y;
+  const int m = blockIdx.z;
+  const int p0 = blockIdx.y * kColChunk;
+  const long lo = (long)m * a.N;
+  const int p1 = min(a.N, p0 + kColChunk);
+  if (blockIdx.x == 0 && p0 + (int)threadIdx.x < p1)
+    a.dw[lo + p0 + threadIdx.x] = a.zv[lo + p0 + threadIdx.x];
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= a.N) return;
-  const long lo = (long)m * a.N;
   const double* Zn = a.Zn + (long)m * a.N * a.N;
-  for (int p = 0; p < a.N; ++p) {
+  for (int p = p0; p < p1; ++p) {
     int q = a.perm[lo + p];
     if (q < 0 || q >= a.N) {
       atomicCAS(a.err, 0, kDevBadShape);
@@ -738,8 +808,6 @@ __global__ void merge_scatter_kernel(LevelArgs a) {
     }
     a.Zw[(lo + r) + (lo + p) * a.ldz] = Zn[r + (long)q * a.N];
   }
-  if (r == 0)
-    for (int p = 0; p < a.N; ++p) a.dw[lo + p] = a.zv[lo + p];
 }
 
 __global__ void finish_kernel(long n, long np, const double* dw, const double* Zw, long ldzw,
@@ -840,7 +908,7 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     dim3 gN(ceil_div_i(a.N, 256), a.nm);
     merge_setup_kernel<<<gN, 256, 0, st>>>(a);
     EVD_LAUNCHED();
-    merge_deflate_kernel<<<a.nm, 32, 0, st>>>(a);
+    merge_deflate_kernel<<<a.nm, kDefThreads, 0, st>>>(a);
     EVD_LAUNCHED();
     hdesc.resize(8 * a.nm);
     EVD_CUDA_TRY(cudaMemcpyAsync(hdesc.data(), a.desc, sizeof(int) * 8 * a.nm,
@@ -861,8 +929,14 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
       merge_rotate_kernel<<<gN, 256, 0, st>>>(a);
       EVD_LAUNCHED();
     }
-    merge_gather_kernel<<<gN, 256, 0, st>>>(a);
-    EVD_LAUNCHED();
+    {
+      const int cols = std::max(Kmax, std::max(a.K12max, a.K23max));
+      if (cols > 0) {
+        dim3 gG(ceil_div_i(a.N, 256), ceil_div_i(cols, kColChunk), a.nm);
+        merge_gather_kernel<<<gG, 256, 0, st>>>(a);
+        EVD_LAUNCHED();
+      }
+    }
     if (Kmax > 0) {
       dim3 gK(ceil_div_i((long)Kmax * 32, 256), a.nm);
       merge_secular_kernel<<<gK, 256, 0, st>>>(a);
@@ -891,11 +965,12 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
         }
       }
     }
-    merge_copy_deflated_kernel<<<gN, 256, 0, st>>>(a);
+    dim3 gC(ceil_div_i(a.N, 256), ceil_div_i(a.N, kColChunk), a.nm);
+    merge_copy_deflated_kernel<<<gC, 256, 0, st>>>(a);
     EVD_LAUNCHED();
     merge_finalize_rank_kernel<<<gN, 256, 0, st>>>(a);
     EVD_LAUNCHED();
-    merge_scatter_kernel<<<gN, 256, 0, st>>>(a);
+    merge_scatter_kernel<<<gC, 256, 0, st>>>(a);
     EVD_LAUNCHED();
   }
   dim3 gf(ceil_div_i(n, 256), (unsigned)std::min<long>(n, 65535));
