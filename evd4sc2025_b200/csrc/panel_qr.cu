@@ -7,8 +7,11 @@
 //
 // Same numerics, B200 structure:
 //  * The TSQR tree has the reference's shape (128-row tiles, R factors
-//    stacked 32 rows per child, fan-in 4), but runs as ONE up-sweep kernel:
-//    each CTA factors its tile in registers/shared memory, publishes its R,
+//    stacked 32 rows per child, fan-in 4; api/inc/TallShinnyQR.h:9-133).  The
+//    shape is kept on purpose: the signs of R (hence of Y, W and the band)
+//    follow from the Householder sign rule applied node by node, so another
+//    tree gives R up to row signs, not the reference's R.  It runs as ONE
+//    up-sweep kernel: each CTA factors its tile in registers, publishes its R,
 //    and the last child to arrive at a parent (atomic counter) goes on to
 //    factor the parent.  Nobody waits, so there is no grid barrier and no
 //    spin.  The reference launches one kernel plus batched GEMMs per level.
@@ -29,9 +32,12 @@ namespace evd {
 
 namespace {
 
-constexpr int kTile = 128;   // rows per TSQR tile (reference: M = 128)
-constexpr int kNB = 32;      // panel width (reference: N = 32)
-constexpr int kThreads = 256;
+constexpr int kTile = 128;        // rows per TSQR tile (reference: M = 128)
+constexpr int kNB = 32;           // panel width (reference: N = 32)
+constexpr int kFan = kTile / kNB; // children per tree node (their R factors fill one tile)
+constexpr int kThreads = 256;     // 8 warps x 4 columns
+constexpr int kRPL = kTile / 32;  // rows per lane in a tile QR
+constexpr int kSub = 128;         // rows per CTA of the finishing kernel
 constexpr int kMaxLevels = 16;
 
 struct TsqrPlan {
@@ -80,35 +86,56 @@ TsqrPlan make_plan(long m) {
   return p;
 }
 
+// Full warp sums of four per-lane partials (one per column of the warp):
+// reduce-scatter (lanes keep two columns, then one) and a broadcast back, 20
+// 32-bit shuffles instead of 40 for four butterflies.
+__device__ __forceinline__ void warp_sum4(double (&p)[4], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8;
+  const double s0 = b4 ? p[0] : p[2], s1 = b4 ? p[1] : p[3];
+  const double r0 = __shfl_xor_sync(0xffffffffu, s0, 16);
+  const double r1 = __shfl_xor_sync(0xffffffffu, s1, 16);
+  const double k0 = (b4 ? p[2] : p[0]) + r0;  // column 2*b4
+  const double k1 = (b4 ? p[3] : p[1]) + r1;  // column 2*b4 + 1
+  const double r = __shfl_xor_sync(0xffffffffu, b3 ? k0 : k1, 8);
+  double k = (b3 ? k1 : k0) + r;  // column 2*b4 + b3
+  k += __shfl_xor_sync(0xffffffffu, k, 4);
+  k += __shfl_xor_sync(0xffffffffu, k, 2);
+  k += __shfl_xor_sync(0xffffffffu, k, 1);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) p[c] = __shfl_sync(0xffffffffu, k, (c >> 1) * 16 + (c & 1) * 8);
+}
+
 // Householder QR of one tile (mm <= 128 rows, 32 columns) held in registers:
-// warp w owns columns 4w..4w+3, lane l owns rows l, l+32, l+64, l+96.
-// Writes R (32x32, upper; diag = -sign(x0)||x||) to Rdst and the explicit thin
-// Q over the tile rows back to src.  Same steps as my_hou_kernel<128,32>.
+// warp w owns columns 4w..4w+3, lane l owns rows l + 32 i (i < 4).  Writes R
+// (32 x 32, upper; diag = -sign(x0) ||x||) to Rdst and leaves the reflectors in
+// the tile (column j, rows >= j; rows above hold R) for tile_form_q.  Same
+// steps as my_hou_kernel<128,32> (util/inc/kernelQR.h:215-414): u = x/||x||,
+// u0 += sign(u0), u scaled to ||u||^2 = 2.  Step j's reflector goes through
+// shared memory to every warp: one barrier per column.
 struct TileSmem {
-  double V[kNB * kTile];  // Householder vectors, column j at V[j*128 ..]
-  double us[kTile];
+  double V[kNB * kTile];  // reflector j at V[j * kTile ..]
   double RR[kNB];
 };
+constexpr size_t kTileSmem = sizeof(TileSmem);
 
-__device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, TileSmem& sm,
-                        double* qtop_copy) {
+__device__ void tile_factor(double* src, long ld, int mm, double* Rdst, long ldR, TileSmem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double a[4][4];
+  double a[4][kRPL];
 #pragma unroll
   for (int c = 0; c < 4; ++c)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int row = lane + 32 * i;
+    for (int i = 0; i < kRPL; ++i) {
+      const int row = lane + 32 * i;
       a[c][i] = (row < mm) ? __ldcg(src + row + (long)(4 * warp + c) * ld) : 0.0;
     }
 
   for (int j = 0; j < kNB; ++j) {
     const int ow = j >> 2, oc = j & 3;
     if (warp == ow) {
-      double x[4], ss = 0.0;
+      double x[kRPL], ss = 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        int row = lane + 32 * i;
+      for (int i = 0; i < kRPL; ++i) {
+        const int row = lane + 32 * i;
         double v = 0.0;
 #pragma unroll
         for (int c = 0; c < 4; ++c)
@@ -116,25 +143,18 @@ __device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, Ti
         x[i] = (row >= j && row < mm) ? v : 0.0;
         ss = fma(x[i], x[i], ss);
       }
-      double nrm2 = warp_sum(ss);
-      double nrm = sqrt(nrm2);
-      double scale = (nrm2 > 0.0) ? 1.0 / nrm : 0.0;
+      const double nrm2 = warp_sum(ss);
+      const double x0 = __shfl_sync(0xffffffffu, x[0], j);  // row j: lane j, i = 0
+      const bool live = nrm2 > 0.0;
+      const double rn = live ? rsqrt(nrm2) : 0.0;  // 1 / ||x||
+      const double u0 = x0 * rn;
+      const double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
+      const double s2 = live ? rsqrt(fabs(u0n)) : 0.0;
+      if (lane == 0) sm.RR[j] = (u0 >= 0.0) ? -(nrm2 * rn) : nrm2 * rn;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) sm.us[lane + 32 * i] = x[i] * scale;
-      __syncwarp();
-      double u0 = sm.us[j];
-      double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
-      double s2 = (nrm2 > 0.0) ? 1.0 / sqrt(fabs(u0n)) : 0.0;
-      if (lane == 0) sm.RR[j] = (u0 >= 0.0) ? -nrm : nrm;
-      __syncwarp();
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        int row = lane + 32 * i;
-        double u = sm.us[row];
-        if (row == j) u = u0n;
-        u *= s2;
-        if (nrm2 == 0.0) u = 0.0;
-        sm.us[row] = u;
+      for (int i = 0; i < kRPL; ++i) {
+        const int row = lane + 32 * i;
+        const double u = ((row == j) ? u0n : x[i] * rn) * s2;
         sm.V[j * kTile + row] = u;
 #pragma unroll
         for (int c = 0; c < 4; ++c)
@@ -142,74 +162,91 @@ __device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, Ti
       }
     }
     __syncthreads();
-    double uv[4];
+    if (4 * warp + 3 <= j) continue;  // all columns of this warp factored (warp-uniform)
+    double uv[kRPL];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) uv[i] = sm.us[lane + 32 * i];
-    // the four column dot products are reduced together (interleaved
-    // butterflies); columns <= j get a zero update
+    for (int i = 0; i < kRPL; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
+    // the four column dot products are reduced together; columns <= j get a
+    // zero update
     double pc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      double p = 0.0;
+      double p0 = 0.0, p1 = 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) p = fma(uv[i], a[c][i], p);
-      pc[c] = p;
+      for (int i = 0; i < kRPL; i += 2) {
+        p0 = fma(uv[i], a[c][i], p0);
+        p1 = fma(uv[i + 1], a[c][i + 1], p1);
+      }
+      pc[c] = p0 + p1;
     }
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) pc[c] += __shfl_xor_sync(0xffffffffu, pc[c], m);
+    warp_sum4(pc, lane);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const double dot = (4 * warp + c > j) ? pc[c] : 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
+      for (int i = 0; i < kRPL; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
     }
-    __syncthreads();
   }
 
-  // R: row k = lane (i = 0), column h = 4w + c
+  // R: row k = lane (i = 0), column h = 4w + c; reflectors back into the tile
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    int h = 4 * warp + c;
-    double r = (lane < h) ? a[c][0] : ((lane == h) ? sm.RR[h] : 0.0);
+    const int h = 4 * warp + c;
+    const double r = (lane < h) ? a[c][0] : ((lane == h) ? sm.RR[h] : 0.0);
     Rdst[lane + (long)h * ldR] = r;
+#pragma unroll
+    for (int i = 0; i < kRPL; ++i) {
+      const int row = lane + 32 * i;
+      if (row < mm) src[row + (long)h * ld] = a[c][i];
+    }
   }
+}
 
-  // explicit thin Q = H_0 ... H_31 I[:, :32], accumulated backwards
-  double q[4][4];
+// Explicit thin Q = H_0 ... H_31 I[:, :32] of a factored tile, from the
+// reflectors left in it, accumulated backwards and written over them.  Before
+// H_j is applied, columns c < j are still e_c, which H_j leaves unchanged, so
+// warps whose columns are all left of j skip the step.
+__device__ void tile_form_q(double* src, long ld, int mm, TileSmem& sm, double* qtop_copy) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int e = threadIdx.x; e < kNB * kTile; e += kThreads) {
+    const int j = e / kTile, row = e % kTile;
+    sm.V[e] = (row >= j && row < mm) ? __ldcg(src + row + (long)j * ld) : 0.0;
+  }
+  __syncthreads();
+  double q[4][kRPL];
 #pragma unroll
   for (int c = 0; c < 4; ++c)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) q[c][i] = (lane + 32 * i == 4 * warp + c) ? 1.0 : 0.0;
+    for (int i = 0; i < kRPL; ++i) q[c][i] = (lane + 32 * i == 4 * warp + c) ? 1.0 : 0.0;
   for (int j = kNB - 1; j >= 0; --j) {
-    double uv[4];
+    if (4 * warp + 3 < j) continue;  // warp-uniform
+    double uv[kRPL];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
+    for (int i = 0; i < kRPL; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
     double pc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      double p = 0.0;
+      double p0 = 0.0, p1 = 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) p = fma(uv[i], q[c][i], p);
-      pc[c] = p;
+      for (int i = 0; i < kRPL; i += 2) {
+        p0 = fma(uv[i], q[c][i], p0);
+        p1 = fma(uv[i + 1], q[c][i + 1], p1);
+      }
+      pc[c] = p0 + p1;
     }
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) pc[c] += __shfl_xor_sync(0xffffffffu, pc[c], m);
+    warp_sum4(pc, lane);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const double dot = (4 * warp + c >= j) ? pc[c] : 0.0;
 #pragma unroll
-      for (int i = 0; i < 4; ++i) q[c][i] = fma(-dot, uv[i], q[c][i]);
+      for (int i = 0; i < kRPL; ++i) q[c][i] = fma(-dot, uv[i], q[c][i]);
     }
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c)
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      int row = lane + 32 * i;
+    for (int i = 0; i < kRPL; ++i) {
+      const int row = lane + 32 * i;
       if (row < mm) {
         src[row + (long)(4 * warp + c) * ld] = q[c][i];
         if (qtop_copy && row < kNB) qtop_copy[row + (4 * warp + c) * kNB] = q[c][i];
@@ -217,10 +254,11 @@ __device__ void tile_qr(double* src, long ld, int mm, double* Rdst, long ldR, Ti
     }
 }
 
-__global__ void __launch_bounds__(kThreads) tsqr_up_kernel(const TsqrPlan plan, double* A,
-                                                           long lda, double* ws, double* Rout,
-                                                           long ldr) {
-  __shared__ TileSmem sm;
+__global__ void __launch_bounds__(kThreads, 1) tsqr_up_kernel(const TsqrPlan plan, double* A,
+                                                              long lda, double* ws, double* Rout,
+                                                              long ldr) {
+  extern __shared__ __align__(16) double up_smem[];
+  TileSmem& sm = *reinterpret_cast<TileSmem*>(up_smem);
   __shared__ int is_last;
   int* cnt = reinterpret_cast<int*>(ws + plan.cnt_off);
   int level = 0, idx = blockIdx.x;
@@ -245,11 +283,10 @@ __global__ void __launch_bounds__(kThreads) tsqr_up_kernel(const TsqrPlan plan, 
       Rdst = ws + plan.soff[level + 1] + (long)idx * kNB;
       ldR = plan.rows[level + 1];
     }
-    double* qtop = (level == 0 && idx == 0) ? ws + plan.qtop_off : nullptr;
-    tile_qr(src, ld, mm, Rdst, ldR, sm, qtop);
+    tile_factor(src, ld, mm, Rdst, ldR, sm);
     if (root) break;
-    const int parent = idx / 4;
-    const int nch = min(4, plan.T[level] - 4 * parent);
+    const int parent = idx / kFan;
+    const int nch = min(kFan, plan.T[level] - kFan * parent);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -264,6 +301,31 @@ __global__ void __launch_bounds__(kThreads) tsqr_up_kernel(const TsqrPlan plan, 
     ++level;
     idx = parent;
   }
+}
+
+// Explicit Q of every tree node, all levels at once (the up-sweep left the
+// reflectors in each node's tile): one CTA per node.
+__global__ void __launch_bounds__(kThreads, 1) tsqr_q_kernel(const TsqrPlan plan, double* A,
+                                                             long lda, double* ws) {
+  extern __shared__ __align__(16) double q_smem[];
+  TileSmem& sm = *reinterpret_cast<TileSmem*>(q_smem);
+  int idx = blockIdx.x, level = 0;
+  while (level < plan.nlev && idx >= plan.T[level]) {
+    idx -= plan.T[level];
+    ++level;
+  }
+  if (level >= plan.nlev) return;
+  double* src;
+  long ld;
+  if (level == 0) {
+    src = A + (long)idx * kTile;
+    ld = lda;
+  } else {
+    src = ws + plan.soff[level] + (long)idx * kTile;
+    ld = plan.rows[level];
+  }
+  const int mm = min(kTile, plan.rows[level] - idx * kTile);
+  tile_form_q(src, ld, mm, sm, (level == 0 && idx == 0) ? ws + plan.qtop_off : nullptr);
 }
 
 struct FinishSmem {
@@ -289,7 +351,7 @@ __device__ void mul32(const double* Bm, const double* M, double* Out) {
 __device__ void path_product(const TsqrPlan& plan, const double* ws, int t, FinishSmem& sm) {
   int idxs[kMaxLevels];
   idxs[0] = t;
-  for (int L = 1; L < plan.nlev; ++L) idxs[L] = idxs[L - 1] / 4;
+  for (int L = 1; L < plan.nlev; ++L) idxs[L] = idxs[L - 1] / kFan;
   for (int e = threadIdx.x; e < kNB * kNB; e += kThreads) {
     int r = e & 31, c = e >> 5;
     sm.M[r * 33 + c] = (r == c) ? 1.0 : 0.0;
@@ -323,21 +385,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                        long ldr, double* Aband, long ldband) {
   extern __shared__ double dsm[];
   __shared__ FinishSmem sm;
-  double* Qs = dsm;                   // 128 x 33 : tile rows of Q (then Y)
-  double* Ws = dsm + kTile * 33;      // 128 x 33 : W rows
+  double* Qs = dsm;                   // 128 x 33 : rows of Q (then Y)
+  double* Ws = dsm + kSub * 33;       // 128 x 33 : W rows
   const int t = blockIdx.x;
-  const int r0 = t * kTile;
-  const int mm = min(kTile, plan.m - r0);
+  const int r0 = t * kSub;
+  const int mm = min(kSub, plan.m - r0);
+  const int leaf = r0 / kTile;       // TSQR leaf tile holding these rows
 
   // tile rows of Q = Qleaf_t * M_t; the leaf Q tile is staged in shared
   // memory (coalesced) before the product
-  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
-    int r = e & (kTile - 1), c = e >> 7;
+  for (int e = threadIdx.x; e < kSub * kNB; e += kThreads) {
+    int r = e & (kSub - 1), c = e >> 7;
     Ws[r * 33 + c] = (r < mm) ? __ldcg(A + (long)(r0 + r) + (long)c * lda) : 0.0;
   }
-  path_product(plan, ws, t, sm);  // ends with __syncthreads
-  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
-    int r = e & (kTile - 1), c = e >> 7;
+  path_product(plan, ws, leaf, sm);  // ends with __syncthreads
+  for (int e = threadIdx.x; e < kSub * kNB; e += kThreads) {
+    int r = e & (kSub - 1), c = e >> 7;
     double s = 0.0;
 #pragma unroll 8
     for (int k = 0; k < kNB; ++k) s = fma(Ws[r * 33 + k], sm.M[k * 33 + c], s);
@@ -346,15 +409,15 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
 
   if (mode == 0) {
-    for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
-      int r = e & (kTile - 1), c = e >> 7;
+    for (int e = threadIdx.x; e < kSub * kNB; e += kThreads) {
+      int r = e & (kSub - 1), c = e >> 7;
       if (r < mm) A[(long)(r0 + r) + (long)c * lda] = Qs[r * 33 + c];
     }
     return;
   }
 
   // LU of (I - Qtop), Qtop = Qleaf_0[0:32] * M_0 (recomputed by every CTA)
-  if (t != 0) path_product(plan, ws, 0, sm);
+  if (leaf != 0) path_product(plan, ws, 0, sm);
   {
     const double* q0 = ws + plan.qtop_off;
     if (t == 0) {
@@ -373,19 +436,26 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
   __syncthreads();
-  // unpivoted LU in place (one warp; lane = row)
+  // unpivoted LU in place (one warp, lane = row, the row in registers; row k
+  // is broadcast by shuffles)
   if (threadIdx.x < 32) {
     const int r = threadIdx.x;
+    double lu[kNB];
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) lu[c] = sm.LU[r * 33 + c];
+#pragma unroll
     for (int k = 0; k < kNB; ++k) {
-      double piv = sm.LU[k * 33 + k];
-      __syncwarp();
-      if (r > k) {
-        double l = sm.LU[r * 33 + k] / piv;
-        sm.LU[r * 33 + k] = l;
-        for (int c = k + 1; c < kNB; ++c) sm.LU[r * 33 + c] = fma(-l, sm.LU[k * 33 + c], sm.LU[r * 33 + c]);
+      const double piv = __shfl_sync(0xffffffffu, lu[k], k);
+      const double l = lu[k] / piv;
+      if (r > k) lu[k] = l;
+#pragma unroll
+      for (int c = k + 1; c < kNB; ++c) {
+        const double ukc = __shfl_sync(0xffffffffu, lu[c], k);
+        if (r > k) lu[c] = fma(-l, ukc, lu[c]);
       }
-      __syncwarp();
     }
+#pragma unroll
+    for (int c = 0; c < kNB; ++c) sm.LU[r * 33 + c] = lu[c];
   }
   __syncthreads();
 
@@ -429,8 +499,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int h = 0; h < kNB; ++h) dst[row * 33 + h] = x[h];
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < kTile * kNB; e += kThreads) {
-    int r = e & (kTile - 1), c = e >> 7;
+  for (int e = threadIdx.x; e < kSub * kNB; e += kThreads) {
+    int r = e & (kSub - 1), c = e >> 7;
     if (r < mm) {
       long gr = r0 + r;
       Yout[gr + (long)c * ldy] = Qs[r * 33 + c];
@@ -444,7 +514,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-constexpr size_t kFinishDyn = 2 * kTile * 33 * sizeof(double);
+constexpr size_t kFinishDyn = 2 * kSub * 33 * sizeof(double);
 
 int finish_attr() {
   static bool done = false;
@@ -452,6 +522,10 @@ int finish_attr() {
     EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_finish_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kFinishDyn));
+    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_up_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTileSmem));
+    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kTileSmem));
     done = true;
   }
   return EVD_SUCCESS;
@@ -479,11 +553,15 @@ int panel_qr_launch(long m, double* A, long lda, double* ws, int mode, double* Y
                     cudaStream_t st) {
   TsqrPlan plan = make_plan(m);
   if (plan.nlev >= kMaxLevels) return EVD_ERR_INVALID_ARG;
-  tsqr_up_kernel<<<plan.T[0], kThreads, 0, st>>>(plan, A, lda, ws, R, ldr);
-  EVD_LAUNCHED();
   EVD_TRY(finish_attr());
-  tsqr_finish_kernel<<<plan.T[0], kThreads, kFinishDyn, st>>>(plan, ws, A, lda, mode, Yout, ldy,
-                                                              Wout, ldw, R, ldr, Aband, ldband);
+  tsqr_up_kernel<<<plan.T[0], kThreads, kTileSmem, st>>>(plan, A, lda, ws, R, ldr);
+  EVD_LAUNCHED();
+  int nodes = 0;
+  for (int l = 0; l < plan.nlev; ++l) nodes += plan.T[l];
+  tsqr_q_kernel<<<nodes, kThreads, kTileSmem, st>>>(plan, A, lda, ws);
+  EVD_LAUNCHED();
+  tsqr_finish_kernel<<<ceil_div_i(m, kSub), kThreads, kFinishDyn, st>>>(
+      plan, ws, A, lda, mode, Yout, ldy, Wout, ldw, R, ldr, Aband, ldband);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
