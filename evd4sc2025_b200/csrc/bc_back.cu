@@ -195,15 +195,13 @@ __global__ void __launch_bounds__(kQThreads)
                seg_off(g, 0) + 2 * t - g);
 }
 
-// One group (segment J) of the current block on the warp's window tiles
-// 4J .. 4J+4: W = X^T Y, W <- W (-T or -T^T), X^T += W Y^T.
-template <int J>
-__device__ __forceinline__ void apply_group(double (&x)[kTiles][4], const double* ys,
-                                            const double* ts, int lane, int offW, int offU0,
-                                            int offU1) {
-  double wa[4] = {0.0, 0.0, 0.0, 0.0}, wb[4] = {0.0, 0.0, 0.0, 0.0};
+// W += X^T Y over tiles i in [i0, i1) of group J (two accumulator chains by
+// tile parity).
+__device__ __forceinline__ void w_part(const double (&x)[kTiles][4], const double* ys, int offW,
+                                       int J, int i0, int i1, double (&wa)[4], double (&wb)[4]) {
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
+    if (i < i0 || i >= i1) continue;
     const int ti = 4 * J + i;
     const double b0 = ys[offW + J * kSeg + 8 * i];
     const double b1 = ys[offW + J * kSeg + 8 * i + 1];
@@ -212,35 +210,48 @@ __device__ __forceinline__ void apply_group(double (&x)[kTiles][4], const double
     else
       mma16(wa, x[ti][0], x[ti][2], x[ti][1], x[ti][3], b0, b1);
   }
-#pragma unroll
-  for (int q = 0; q < 4; ++q) wa[q] += wb[q];
-  double wt[4] = {0.0, 0.0, 0.0, 0.0};
-  const double2 tf = *reinterpret_cast<const double2*>(ts + J * 64 + lane * 2);
-  mma16(wt, wa[0], wa[2], wa[1], wa[3], tf.x, tf.y);
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const int ti = 4 * J + i;
-    const double b0 = ys[offU0 + J * kSeg + 8 * i];
-    const double b1 = ys[offU1 + J * kSeg + 8 * i];
-    mma16(x[ti], wt[0], wt[2], wt[1], wt[3], b0, b1);
-  }
 }
 
-// First and second half of a block: segments 3,2 then 1,0 (forward) or 0,1
-// then 2,3 (reverse).
+// One block: its 4 groups in dependency order (segments 3..0 forward, 0..3
+// reverse), each W = X^T Y, W <- W (-T or -T^T), X^T += W Y^T.  Consecutive
+// groups share one tile (forward: tile 4J = the next group's last tile;
+// reverse: tile 4J+4 = the next group's first), so the next group's W over
+// its other four tiles is issued between this group's T product and its
+// update, and the shared tile is updated first.
 template <bool FWD>
-__device__ __forceinline__ void apply_groups_lo(double (&x)[kTiles][4], const double* ys,
-                                                const double* ts, int lane, int offW, int offU0,
-                                                int offU1) {
-  apply_group<FWD ? 3 : 0>(x, ys, ts, lane, offW, offU0, offU1);
-  apply_group<FWD ? 2 : 1>(x, ys, ts, lane, offW, offU0, offU1);
-}
-template <bool FWD>
-__device__ __forceinline__ void apply_groups_hi(double (&x)[kTiles][4], const double* ys,
-                                                const double* ts, int lane, int offW, int offU0,
-                                                int offU1) {
-  apply_group<FWD ? 1 : 2>(x, ys, ts, lane, offW, offU0, offU1);
-  apply_group<FWD ? 0 : 3>(x, ys, ts, lane, offW, offU0, offU1);
+__device__ __forceinline__ void apply_block(double (&x)[kTiles][4], const double* ys,
+                                            const double* ts, int lane, int offW, int offU0,
+                                            int offU1) {
+  double wa[4] = {0.0, 0.0, 0.0, 0.0}, wb[4] = {0.0, 0.0, 0.0, 0.0};
+  w_part(x, ys, offW, FWD ? kGroups - 1 : 0, 0, 5, wa, wb);
+#pragma unroll
+  for (int s = 0; s < kGroups; ++s) {
+    const int J = FWD ? kGroups - 1 - s : s;
+    const int JN = FWD ? J - 1 : J + 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) wa[q] += wb[q];
+    double wt[4] = {0.0, 0.0, 0.0, 0.0};
+    const double2 tf = *reinterpret_cast<const double2*>(ts + J * 64 + lane * 2);
+    mma16(wt, wa[0], wa[2], wa[1], wa[3], tf.x, tf.y);
+    double na[4] = {0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
+    if (s + 1 < kGroups) w_part(x, ys, offW, JN, FWD ? 0 : 1, FWD ? 4 : 5, na, nb);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const int i = FWD ? k : 4 - k;  // shared tile first
+      const int ti = 4 * J + i;
+      const double b0 = ys[offU0 + J * kSeg + 8 * i];
+      const double b1 = ys[offU1 + J * kSeg + 8 * i];
+      mma16(x[ti], wt[0], wt[2], wt[1], wt[3], b0, b1);
+    }
+    if (s + 1 < kGroups) {
+      w_part(x, ys, offW, JN, FWD ? 4 : 0, FWD ? 5 : 1, na, nb);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        wa[q] = na[q];
+        wb[q] = nb[q];
+      }
+    }
+  }
 }
 
 // Window tile i of a frame starting at row `base`: rows base+8i .. base+8i+7.
@@ -350,11 +361,10 @@ __global__ void __launch_bounds__(kQThreads, 2)
       load_tile(inc, io, FWD ? (base + 8 * kTiles) : (base - 8), n);
       const double* ys = Ys + (it % 3) * kYBuf;
       const double* ts = Ts + (PRE ? (it % 3) : (it & 1)) * kTBuf;
-      apply_groups_lo<FWD>(x, ys, ts, lane, offW, offU0, offU1);
       if (!PRE && it + 1 < nblk)
         build_t<FWD>(Ys + ((it + 1) % 3) * kYBuf, Ts + ((it + 1) & 1) * kTBuf, gs, warp, lane,
                      offW);
-      apply_groups_hi<FWD>(x, ys, ts, lane, offW, offU0, offU1);
+      apply_block<FWD>(x, ys, ts, lane, offW, offU0, offU1);
       // slide the window one tile: the tile leaving it is final for this strip
       if (FWD) {
         store_tile(x[0], io, base, n);
