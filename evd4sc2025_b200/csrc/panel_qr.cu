@@ -145,12 +145,16 @@ __device__ void tile_factor(double* src, long ld, int mm, double* Rdst, long ldR
       }
       const double nrm2 = warp_sum(ss);
       const double x0 = __shfl_sync(0xffffffffu, x[0], j);  // row j: lane j, i = 0
+      // A zero column (nothing to annihilate) gets u = sqrt(2) e_j rather than
+      // u = 0: H = I - u u^T then only flips row j, R_jj = 0, every reflector
+      // keeps ||u||^2 = 2, and I - Q stays nonsingular for the Householder
+      // reconstruction (u = 0 would give a zero pivot there).
       const bool live = nrm2 > 0.0;
       const double rn = live ? rsqrt(nrm2) : 0.0;  // 1 / ||x||
       const double u0 = x0 * rn;
-      const double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
-      const double s2 = live ? rsqrt(fabs(u0n)) : 0.0;
-      if (lane == 0) sm.RR[j] = (u0 >= 0.0) ? -(nrm2 * rn) : nrm2 * rn;
+      const double u0n = live ? u0 + ((u0 >= 0.0) ? 1.0 : -1.0) : 1.4142135623730951;
+      const double s2 = live ? rsqrt(fabs(u0n)) : 1.0;
+      if (lane == 0) sm.RR[j] = live ? ((u0 >= 0.0) ? -(nrm2 * rn) : nrm2 * rn) : 0.0;
 #pragma unroll
       for (int i = 0; i < kRPL; ++i) {
         const int row = lane + 32 * i;

@@ -1,0 +1,321 @@
+"""Batched uneven-size solves and a continuous-batching serving loop.
+
+Both sit on the plain FP64 solver (``evd_syevd``).  The reference solves one
+matrix per process (``myEVD n b nb``, src/EVD/myEVD.cu:251-706, n a multiple
+of 1024); this layer adds:
+
+* **any n >= 1**: a matrix whose order is not a multiple of 32 is padded to
+  n' = 32 * ceil(n / 32) (at least 64) with a diagonal block placed above the
+  spectrum of A (values 2 s, 2 s + s/k, ... with s >= ||A||_2).  The padded
+  matrix is block diagonal, so its n smallest eigenvalues are those of A and
+  the leading n x n block of the eigenvectors holds A's eigenvectors;
+  nb = 32 * 2^k is the largest such divisor of n' up to 1024.
+* **overlap on the device**: a pool of workers, each with its own CUDA
+  stream, one grow-only workspace and padded buffer pair, and a host thread
+  (the solver synchronises its own stream a few times per solve; ctypes
+  releases the GIL during the call, so the workers' solves overlap on the
+  GPU).
+* **continuous batching** (:class:`Server`): requests arrive over time; a
+  request is admitted when its device footprint fits the memory budget, runs
+  as soon as a worker is free, and its memory is returned when it completes,
+  so requests that arrive while others are on the GPU are admitted as memory
+  frees up.  Latency = completion - arrival; the server reports solves/s and
+  p50/p99 latency.
+
+Every request is served by the FP64 solver, so FP32-tolerance requests get
+FP64 accuracy (the mixed-precision path is not part of this library).
+"""
+from __future__ import annotations
+
+import heapq
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Callable
+
+import torch
+
+from . import F64, _cm, _ptr, _stream, call, empty_cm, lib
+
+MAX_NB = 1024
+
+
+def padded_shape(n: int) -> tuple[int, int]:
+    """(n', nb) for a matrix of order n: n' = 32 * ceil(n/32) (>= 64) and nb
+    the largest 32 * 2^k dividing n', at most 1024."""
+    if n < 1:
+        raise ValueError("matrix order must be >= 1")
+    np_ = max(64, 32 * math.ceil(n / 32))
+    q = np_ // 32
+    nb = 32
+    while nb * 2 <= MAX_NB and q % 2 == 0:
+        nb *= 2
+        q //= 2
+    return np_, nb
+
+
+def footprint_bytes(n: int) -> int:
+    """Device bytes one solve of order n holds: workspace + padded A and X + w."""
+    np_, nb = padded_shape(n)
+    return int(lib().evd_syevd_work_size(np_, 32, nb)) + 2 * np_ * np_ * 8 + np_ * 8
+
+
+class StreamSolver:
+    """One worker: a CUDA stream, one grow-only workspace and one pair of
+    padded A/X buffers (a smaller problem uses the leading block of the
+    buffers, with their leading dimension), so a worker holds at most the
+    footprint of the largest problem it has solved."""
+
+    def __init__(self, device="cuda"):
+        self.device = torch.device(device)
+        self.stream = torch.cuda.Stream(device=self.device)
+        self._ws = None
+        self._wsbytes = 0
+        self._ld = 0
+        self._A = self._X = self._w = None
+
+    def _ensure(self, np_: int, nb: int):
+        need = int(lib().evd_syevd_work_size(np_, 32, nb))
+        if need <= 0:
+            raise ValueError(f"unsupported padded order {np_} (nb {nb})")
+        if need > self._wsbytes:
+            self._ws = None
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+            self._wsbytes = need
+        if np_ > self._ld:
+            self._A = self._X = self._w = None
+            self._A = empty_cm(np_, np_, device=self.device)
+            self._X = empty_cm(np_, np_, device=self.device)
+            self._w = torch.empty(np_, dtype=F64, device=self.device)
+            self._ld = np_
+        return self._A[:np_, :np_], self._X[:np_, :np_], self._w[:np_]
+
+    def release(self):
+        """Drop the workspace and buffers (their memory returns to torch)."""
+        self._ws = self._A = self._X = self._w = None
+        self._wsbytes = self._ld = 0
+
+    def solve(self, A: torch.Tensor):
+        """Eigenvalues (ascending, length n) and eigenvectors (n x n,
+        column-major) of the symmetric FP64 matrix A on this worker's stream.
+        A may live on the host or the device; results are on the device."""
+        n = A.shape[0]
+        np_, nb = padded_shape(n)
+        with torch.cuda.stream(self.stream):
+            Ap, Xp, wp = self._ensure(np_, nb)
+            Ap.zero_()
+            Ap[:n, :n].copy_(A, non_blocking=True)
+            if np_ > n:
+                s = float(torch.linalg.matrix_norm(Ap[:n, :n], ord=1))
+                s = max(s, 1e-300)
+                k = np_ - n
+                pad = 2.0 * s + s * torch.arange(k, dtype=F64, device=self.device) / k
+                Ap[n:, n:].diagonal().copy_(pad)
+            pa, lda = _cm(Ap, "A")
+            px, ldx = _cm(Xp, "X")
+            call("evd_syevd", np_, 32, nb, pa, lda, _ptr(wp), px, ldx, _ptr(self._ws),
+                 self._wsbytes, 0, _stream(self.stream))
+            w = wp[:n].clone()
+            X = empty_cm(n, n, device=self.device)
+            X.copy_(Xp[:n, :n])
+        return w, X
+
+
+def syevd_any(A: torch.Tensor, solver: StreamSolver | None = None):
+    """Eigenpairs of a symmetric FP64 matrix of any order (padded as above)."""
+    solver = solver or StreamSolver(A.device if A.is_cuda else "cuda")
+    w, X = solver.solve(A)
+    solver.stream.synchronize()
+    return w, X
+
+
+def syevd_batched(mats: list[torch.Tensor], nstreams: int = 8, device="cuda",
+                  solvers: list[StreamSolver] | None = None):
+    """Eigenpairs of many symmetric matrices of uneven sizes, solved
+    concurrently on ``nstreams`` streams.  Returns a list of (w, X) in input
+    order (on the device) and the device time of the whole batch in ms
+    (CUDA events: one start event that every stream waits on, one end event
+    per stream; the maximum elapsed time)."""
+    solvers = solvers or [StreamSolver(device) for _ in range(nstreams)]
+    order = sorted(range(len(mats)), key=lambda i: -mats[i].shape[0])  # largest first
+    out: list = [None] * len(mats)
+    nxt = iter(order)
+    lock = threading.Lock()
+    errors: list[BaseException] = []
+    start = torch.cuda.Event(enable_timing=True)
+    start.record(torch.cuda.current_stream(solvers[0].device))
+    ends = []
+
+    def worker(sv: StreamSolver):
+        sv.stream.wait_event(start)
+        try:
+            while True:
+                with lock:
+                    i = next(nxt, None)
+                if i is None:
+                    break
+                out[i] = sv.solve(mats[i])
+        except BaseException as e:  # surfaced to the caller below
+            errors.append(e)
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record(sv.stream)
+        with lock:
+            ends.append(ev)
+
+    threads = [threading.Thread(target=worker, args=(sv,)) for sv in solvers]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    for ev in ends:
+        ev.synchronize()
+    ms = max(start.elapsed_time(ev) for ev in ends) if ends else 0.0
+    return out, ms
+
+
+# ------------------------------------------------------------------- serving
+@dataclass(order=True)
+class Request:
+    arrival: float                       # seconds from the start of the stream
+    rid: int
+    A: torch.Tensor = field(compare=False)
+    tol: str = field(default="fp64", compare=False)   # "fp64" or "fp32"
+    bytes: int = field(default=0, compare=False)
+
+
+@dataclass
+class Result:
+    rid: int
+    n: int
+    arrival: float
+    admitted: float
+    done: float
+    w: torch.Tensor
+    X: torch.Tensor
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+
+class Server:
+    """Continuous-batching request loop over a pool of stream workers.
+
+    ``submit_stream(requests)`` replays requests at their arrival times (seconds
+    after start).  A request is admitted when its device footprint fits under
+    ``budget_bytes`` next to the requests already admitted, then waits for a
+    free worker; its footprint is returned when its solve completes.  Results
+    keep the eigenpairs on the host (``to_host``) or the device.
+
+    ``solve_fn(worker_index, A) -> (w, X)`` and ``footprint_fn(n)`` can be
+    replaced (the tests drive the admission logic without a GPU).  The budget
+    bounds the sum of the footprints of admitted requests; each worker also
+    keeps the buffers of the largest problem it has solved, so the device
+    holds at most that sum plus one largest footprint per worker.
+    """
+
+    def __init__(self, nworkers: int = 8, budget_bytes: int = 150 * 10**9, device="cuda",
+                 solve_fn: Callable | None = None, footprint_fn: Callable | None = None,
+                 to_host: bool = True):
+        self.nworkers = nworkers
+        self.budget = budget_bytes
+        self.to_host = to_host
+        self.footprint_fn = footprint_fn or footprint_bytes
+        if solve_fn is None:
+            self._solvers = [StreamSolver(device) for _ in range(nworkers)]
+
+            def solve_fn(k, A):
+                w, X = self._solvers[k].solve(A)
+                if self.to_host:
+                    w, X = w.cpu(), X.cpu()  # synchronises the worker's stream
+                else:
+                    self._solvers[k].stream.synchronize()
+                return w, X
+        self.solve_fn = solve_fn
+        self._cv = threading.Condition()
+        self._in_use = 0
+        self._ready: list = []          # admitted, waiting for a worker (FIFO by arrival)
+        self._results: list[Result] = []
+        self._closed = False
+        self.max_in_flight_bytes = 0
+
+    def _worker(self, k: int, t0: float):
+        while True:
+            with self._cv:
+                while not self._ready and not self._closed:
+                    self._cv.wait()
+                if not self._ready:
+                    return
+                _, _, req, t_adm = heapq.heappop(self._ready)
+            w, X = self.solve_fn(k, req.A)
+            t_done = time.perf_counter() - t0
+            with self._cv:
+                self._in_use -= req.bytes
+                self._results.append(Result(req.rid, req.A.shape[0], req.arrival, t_adm, t_done,
+                                            w, X))
+                self._cv.notify_all()
+
+    def run(self, requests: list[Request]) -> dict:
+        """Serve the stream; returns throughput and latency statistics."""
+        reqs = sorted(requests)
+        for r in reqs:
+            r.bytes = int(self.footprint_fn(r.A.shape[0]))
+            if r.bytes > self.budget:
+                raise ValueError(f"request {r.rid} (n={r.A.shape[0]}) needs {r.bytes} bytes, "
+                                 f"more than the budget {self.budget}")
+        t0 = time.perf_counter()
+        workers = [threading.Thread(target=self._worker, args=(k, t0)) for k in range(self.nworkers)]
+        for th in workers:
+            th.start()
+        for r in reqs:
+            # replay the arrival time, then wait for memory
+            delay = r.arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            with self._cv:
+                while self._in_use + r.bytes > self.budget:
+                    self._cv.wait()
+                self._in_use += r.bytes
+                self.max_in_flight_bytes = max(self.max_in_flight_bytes, self._in_use)
+                t_adm = time.perf_counter() - t0
+                heapq.heappush(self._ready, (r.arrival, r.rid, r, t_adm))
+                self._cv.notify_all()
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        for th in workers:
+            th.join()
+        wall = time.perf_counter() - t0
+        lat = sorted(res.latency for res in self._results)
+
+        def pct(p):
+            if not lat:
+                return float("nan")
+            return lat[min(len(lat) - 1, int(math.ceil(p / 100.0 * len(lat))) - 1)]
+        return {"requests": len(self._results), "wall_s": wall,
+                "solves_per_s": len(self._results) / wall if wall > 0 else float("nan"),
+                "p50_s": pct(50), "p99_s": pct(99), "max_in_flight_bytes": self.max_in_flight_bytes}
+
+    @property
+    def results(self) -> list[Result]:
+        return sorted(self._results, key=lambda r: r.rid)
+
+
+def poisson_stream(count: int, rate_per_s: float, n_lo: int, n_hi: int, seed: int = 0,
+                   fp64_fraction: float = 0.7) -> list[Request]:
+    """Seeded Poisson arrivals; n log-uniform on [n_lo, n_hi]; symmetrised
+    Gaussian matrices on the host."""
+    g = torch.Generator().manual_seed(seed)
+    t = 0.0
+    reqs = []
+    for i in range(count):
+        t += float(-math.log(1.0 - torch.rand(1, generator=g).item()) / rate_per_s)
+        u = torch.rand(1, generator=g).item()
+        n = int(round(math.exp(math.log(n_lo) + u * (math.log(n_hi) - math.log(n_lo)))))
+        G = torch.randn(n, n, generator=g, dtype=F64)
+        tol = "fp64" if torch.rand(1, generator=g).item() < fp64_fraction else "fp32"
+        reqs.append(Request(t, i, 0.5 * (G + G.t()), tol))
+    return reqs

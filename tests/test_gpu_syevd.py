@@ -67,3 +67,29 @@ def test_syevd_repeatable_and_timed(cuda, evdlib):
     torch.cuda.synchronize()
     assert torch.equal(w1, w2) and torch.equal(X1, X2)  # deterministic
     assert t["total"] > 0 and all(v >= 0 for v in t.values())
+
+
+@pytest.mark.parametrize("kind", ["diagonal", "block_diagonal", "tridiagonal"])
+def test_structured_inputs(cuda, evdlib, kind):
+    """Inputs whose panels are (partly) zero below the band: the panel
+    factorisation must not break down (zero columns get the reflector
+    sqrt(2) e_j)."""
+    n = 256
+    rng = np.random.default_rng(5)
+    if kind == "diagonal":
+        A = np.diag(rng.standard_normal(n))
+    elif kind == "block_diagonal":
+        A = np.zeros((n, n))
+        G = rng.standard_normal((100, 100))
+        A[:100, :100] = 0.5 * (G + G.T)
+        A[100:, 100:] = np.diag(np.linspace(3.0, 4.0, n - 100))
+    else:
+        d, e = rng.standard_normal(n), rng.standard_normal(n - 1)
+        A = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
+    w, X = evdlib.syevd(Ad, 32, 64)
+    res, orth = evdlib.check_eig(Ad, w, X)
+    torch.cuda.synchronize()
+    w_ref = np.linalg.eigvalsh(A)
+    assert np.abs(w.cpu().numpy() - w_ref).max() <= 1e-12 * np.abs(A).max() * 8
+    assert res <= 1e-13 and orth <= 1e-13, (res, orth)

@@ -1,0 +1,84 @@
+"""Host logic of the batched/serving layer (no GPU): padding rule, admission
+under a memory budget, FIFO service, latency statistics."""
+import threading
+import time
+
+import pytest
+import torch
+
+pytest.importorskip("evd4sc2025_b200")
+from evd4sc2025_b200 import serve  # noqa: E402
+
+
+@pytest.mark.parametrize("n,np_,nb", [(1, 64, 64), (64, 64, 64), (65, 96, 32), (100, 128, 128),
+                                      (1000, 1024, 1024), (1025, 1056, 32), (3000, 3008, 64),
+                                      (8192, 8192, 1024), (16384, 16384, 1024)])
+def test_padded_shape(n, np_, nb):
+    assert serve.padded_shape(n) == (np_, nb)
+    assert np_ % nb == 0 and (nb // 32) & (nb // 32 - 1) == 0
+
+
+def test_padding_keeps_the_spectrum():
+    """The padded block-diagonal matrix has A's eigenpairs as its n smallest."""
+    g = torch.Generator().manual_seed(3)
+    n = 45
+    G = torch.randn(n, n, generator=g, dtype=torch.float64)
+    A = 0.5 * (G + G.t())
+    np_, _ = serve.padded_shape(n)
+    s = float(torch.linalg.matrix_norm(A, ord=1))
+    k = np_ - n
+    P = torch.zeros(np_, np_, dtype=torch.float64)
+    P[:n, :n] = A
+    P[n:, n:] = torch.diag(2 * s + s * torch.arange(k, dtype=torch.float64) / k)
+    w_p, X_p = torch.linalg.eigh(P)
+    w_a = torch.linalg.eigvalsh(A)
+    assert torch.allclose(w_p[:n], w_a, atol=1e-12 * s)
+    assert float(X_p[n:, :n].abs().max()) <= 1e-12
+
+
+def _fake_requests(sizes, gap=0.002):
+    return [serve.Request(i * gap, i, torch.zeros(n, n, dtype=torch.float64))
+            for i, n in enumerate(sizes)]
+
+
+def test_admission_respects_budget_and_serves_everything():
+    in_flight = {"now": 0, "max": 0}
+    lock = threading.Lock()
+
+    def solve(k, A):
+        n = A.shape[0]
+        with lock:
+            in_flight["now"] += n
+            in_flight["max"] = max(in_flight["max"], in_flight["now"])
+        time.sleep(0.004)
+        with lock:
+            in_flight["now"] -= n
+        return torch.zeros(n), torch.zeros(n, n)
+
+    sizes = [30, 50, 20, 70, 10, 40, 60, 25, 35, 45]
+    srv = serve.Server(nworkers=4, budget_bytes=100, solve_fn=solve, footprint_fn=lambda n: n)
+    stats = srv.run(_fake_requests(sizes))
+    assert stats["requests"] == len(sizes)
+    assert srv.max_in_flight_bytes <= 100
+    assert in_flight["max"] <= 100
+    res = srv.results
+    assert [r.rid for r in res] == list(range(len(sizes)))
+    for r in res:
+        assert r.admitted >= r.arrival - 1e-6 and r.done >= r.admitted
+    assert stats["p50_s"] <= stats["p99_s"]
+
+
+def test_oversized_request_is_rejected():
+    srv = serve.Server(nworkers=1, budget_bytes=10, solve_fn=lambda k, A: (None, None),
+                       footprint_fn=lambda n: n)
+    with pytest.raises(ValueError):
+        srv.run(_fake_requests([5, 11]))
+
+
+def test_poisson_stream_is_seeded():
+    a = serve.poisson_stream(20, 100.0, 64, 256, seed=5)
+    b = serve.poisson_stream(20, 100.0, 64, 256, seed=5)
+    assert [r.A.shape[0] for r in a] == [r.A.shape[0] for r in b]
+    assert all(64 <= r.A.shape[0] <= 256 for r in a)
+    assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
+    assert torch.equal(a[3].A, b[3].A) and torch.equal(a[3].A, a[3].A.t())
