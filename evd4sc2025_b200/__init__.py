@@ -372,6 +372,36 @@ def syevd(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | None = N
 myEVD = syevd
 
 
+def syevd_values(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | None = None,
+                 timed: bool = False, stream=None, w: torch.Tensor | None = None) -> torch.Tensor:
+    """Eigenvalues only (ascending) of the symmetric FP64 matrix A: stage 1,
+    the chase without reflectors, Sturm-count multisection; no vectors."""
+    n = A.shape[0]
+    dev = A.device
+    if ws is None or ws.key != (n, b, nb):
+        ws = Workspace(n, b, nb, device=dev)
+    if w is None:
+        w = torch.empty(n, dtype=F64, device=dev)
+    pa, lda = _cm(A, "A")
+    call("evd_syevd_values", n, b, nb, pa, lda, _ptr(w), _ptr(ws.buf), ws.nbytes,
+         1 if timed else 0, _stream(stream))
+    return w
+
+
+eigvalsh = syevd_values
+
+
+def stebz(d: torch.Tensor, e: torch.Tensor, stream=None) -> torch.Tensor:
+    """Eigenvalues (ascending) of the symmetric tridiagonal (d, e), no vectors."""
+    n = d.shape[0]
+    w = torch.empty(n, dtype=F64, device=d.device)
+    nw = max(1, lib().evd_stebz_work_size(n))
+    work = torch.empty(nw, dtype=F64, device=d.device)
+    ep = _ptr(e) if e.numel() > 0 else None
+    call("evd_stebz", n, _ptr(d), ep, _ptr(w), _ptr(work), nw, _stream(stream))
+    return w
+
+
 def fp64_peak_tflops(stream=None) -> float:
     """Measured FP64 DMMA peak of this GPU (TFLOP/s)."""
     out = (C.c_double * 1)()

@@ -51,6 +51,9 @@ SIGNATURES = {
     "evd_check_eig": (_i, [_l, _p, _l, _p, _p, _l, _p, _p, _p]),
     "evd_syevd_work_size": (_l, [_l, _l, _l]),
     "evd_syevd_last_timings": (None, [_p]),
+    "evd_stebz_work_size": (_l, [_l]),
+    "evd_stebz": (_i, [_l, _p, _p, _p, _p, _l, _p]),
+    "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
 }
 

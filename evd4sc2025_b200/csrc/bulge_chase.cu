@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kChaseThreads)
           u *= 1.0 / sqrt(fabs(u0n));
         }
         sm.u[lane] = u;
-        if (lane < rb) U[(r + lane) + (long)s * ldU] = u;
+        if (U != nullptr && lane < rb) U[(r + lane) + (long)s * ldU] = u;
       }
       __syncthreads();
 
@@ -322,11 +322,11 @@ long chase_iwork_ints(long n) { return n + 64; }
 // 16-byte aligned dSub.
 int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
                       double* d, double* e, int* iwork, cudaStream_t st) {
-  if (n < 0 || b != kBW || ldSub != 2 * b || (n > 0 && ldU < n)) return EVD_ERR_INVALID_ARG;
+  if (n < 0 || b != kBW || ldSub != 2 * b || (dU && n > 0 && ldU < n)) return EVD_ERR_INVALID_ARG;
   if (((uintptr_t)dSub & 15u) != 0) return EVD_ERR_INVALID_ARG;
   if (n > (1L << 30)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
-  if (!dSub || !d || !iwork || (n > 2 && !dU) || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;
+  if (!dSub || !d || !iwork || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;  // dU may be NULL
   int* prog = iwork;
   int* ticket = iwork + n;
   int* err = iwork + n + 32;

@@ -32,6 +32,7 @@ long chase_iwork_ints(long n);
 int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU, double* d,
                       double* e, int* iwork, cudaStream_t st);
 long stedc_ws_doubles(long n);
+int stebz(long n, const double* d, const double* e, double* w, double* work, cudaStream_t st);
 long stedc_ws_ints(long n);
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
           long liwork, cudaStream_t st);
@@ -152,6 +153,53 @@ int syevd(long n, long b, long nb, const double* A, long lda, double* w, double*
 
 size_t syevd_ws_bytes(long n, long b, long nb) { return layout(n, b, nb).bytes; }
 
+// Eigenvalues only: stage 1, the chase without storing reflectors, and
+// Sturm-count multisection on the tridiagonal (no vectors, no back
+// transformation).  Same workspace as syevd.
+int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
+                 long lwork_bytes, int timed, cudaStream_t st) {
+  if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
+  if (lda < n || !A || !w || !work) return EVD_ERR_INVALID_ARG;
+  SyevdLayout L = layout(n, b, nb);
+  if ((size_t)lwork_bytes < L.bytes) return EVD_ERR_WORKSPACE;
+  double* base = reinterpret_cast<double*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  int* ibase = reinterpret_cast<int*>(base + L.end_d);
+  double *OA = base + L.oOA, *dA = base + L.oA, *W = base + L.oW, *Y = base + L.oY,
+         *Z = base + L.oZ, *R = base + L.oR, *S = base + L.oS, *sub = base + L.oSub,
+         *d = base + L.oD, *e = base + L.oE, *SW = base + L.oStedc;
+  int* ich = ibase + L.oIchase;
+  cudaEvent_t ev[4];
+  if (timed) {
+    for (auto& x : ev) EVD_CUDA_TRY(cudaEventCreate(&x));
+    EVD_CUDA_TRY(cudaEventRecord(ev[0], st));
+  }
+  EVD_TRY(copy_matrix(n, n, A, lda, OA, n, st));
+  EVD_TRY(copy_matrix(n, n, A, lda, dA, n, st));
+  EVD_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * n * n, st));
+  EVD_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * n * n, st));
+  EVD_TRY(sy2sb(n, n, b, nb, OA, n, dA, n, W, n, Y, n, Z, n, R, n, S,
+                (long)sy2sb_ws_doubles(n, b, nb), st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[1], st));
+  EVD_TRY(band_pack(n, b, dA, n, sub, 2 * b, st));
+  EVD_TRY(bulge_chase_async(n, b, sub, 2 * b, nullptr, n, d, e, ich, st));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[2], st));
+  EVD_TRY(stebz(n, d, e, w, SW, st));
+  if (timed) {
+    EVD_CUDA_TRY(cudaEventRecord(ev[3], st));
+    EVD_CUDA_TRY(cudaEventSynchronize(ev[3]));
+    float ms;
+    for (int i = 0; i < 3; ++i) {
+      EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+      g_timings[i] = ms;
+    }
+    g_timings[3] = g_timings[4] = 0.0;
+    EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[3]));
+    g_timings[5] = ms;
+    for (auto& x : ev) cudaEventDestroy(x);
+  }
+  return read_device_error(ich + n + 32, st);
+}
+
 }  // namespace evd
 
 extern "C" long evd_syevd_work_size(long n, long b, long nb) {
@@ -161,6 +209,11 @@ extern "C" long evd_syevd_work_size(long n, long b, long nb) {
 
 extern "C" void evd_syevd_last_timings(double out_ms[6]) {
   for (int i = 0; i < 6; ++i) out_ms[i] = evd::g_timings[i];
+}
+
+extern "C" int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w,
+                                void* work, long lwork_bytes, int timed, cudaStream_t stream) {
+  return evd::syevd_values(n, b, nb, A, lda, w, work, lwork_bytes, timed, stream);
 }
 
 extern "C" int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X,

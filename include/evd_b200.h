@@ -128,7 +128,8 @@ long evd_bulge_chase_iwork_size(long n);
  * (clear it first, as the reference does at src/EVD/myEVD.cu:413).  d (n) and
  * e (n-1) receive the tridiagonal (kernel_bugle_chasing_cpydSubA2dA +
  * cpyATr2Vector, src/EVD/myEVD.cu:105-123, :477-480).  iwork: evd_bulge_chase_iwork_size
- * bytes of device memory.  b must be 32. */
+ * bytes of device memory.  b must be 32.  dU may be NULL: the reflectors are
+ * then not stored (eigenvalues-only use). */
 int evd_bulge_chase(long n, long b, double* dSub, long ldSub, double* dU, long ldU,
                     double* d, double* e, int* iwork, cudaStream_t stream);
 
@@ -157,6 +158,15 @@ long evd_stedc_iwork_size(long n);  /* ints    */
  * conquer.  d and e are device arrays; e is destroyed. */
 int evd_stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork,
               int* iwork, long liwork, cudaStream_t stream);
+
+/* All eigenvalues (ascending, into w) of the symmetric tridiagonal (d, e), no
+ * vectors: Sturm-count multisection with the pivot rule of LAPACK dstebz.  The
+ * eigenvalues-only counterpart of the reference's LAPACKE_dstedc('I') call
+ * (src/EVD/myEVD.cu:529), which always forms vectors.  work: evd_stebz_work_size
+ * doubles.  d and e are not modified. */
+long evd_stebz_work_size(long n);
+int evd_stebz(long n, const double* d, const double* e, double* w, double* work, long lwork,
+              cudaStream_t stream);
 
 /* ---- Back transformations ----------------------------------------------- */
 
@@ -235,6 +245,15 @@ void evd_syevd_last_timings(double out_ms[6]);
  * stage-2 then stage-1 back transformation.  work: evd_syevd_work_size bytes. */
 int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X,
               long ldX, void* work, long lwork_bytes, int timed, cudaStream_t stream);
+
+/* Eigenvalues only (ascending, device, n) of the symmetric A: sy2sb, the chase
+ * without storing reflectors, and evd_stebz; no back transformation.  The
+ * reference driver has no such mode (its eigenvalues come from the full
+ * dstedc at src/EVD/myEVD.cu:465-491).  work: evd_syevd_work_size bytes;
+ * evd_syevd_last_timings gives [0] sy2sb, [1] chasing, [2] tridiagonal
+ * eigenvalues, [5] total. */
+int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
+                     long lwork_bytes, int timed, cudaStream_t stream);
 
 #ifdef __cplusplus
 }
