@@ -371,6 +371,48 @@ def run_batched(args) -> int:
     return 0
 
 
+def run_values(args) -> int:
+    """Eigenvalues only at the headline size: device time per solve."""
+    import torch
+
+    import evd4sc2025_b200 as evd
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    n, nb = args.n, args.nb
+    stream = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device=dev).manual_seed(1234)
+        G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
+        A = evd.empty_cm(n, n, device=dev)
+        A.copy_(0.5 * (G + G.t()))
+        del G
+        ws = evd.Workspace(n, 32, nb, device=dev)
+        w = torch.empty(n, dtype=torch.float64, device=dev)
+        for _ in range(args.warmup):
+            evd.syevd_values(A, 32, nb, ws=ws, w=w, stream=stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stage_sum = {}
+        e0.record(stream)
+        for _ in range(args.steps):
+            evd.syevd_values(A, 32, nb, ws=ws, w=w, timed=True, stream=stream)
+            for k, v in evd.last_timings().items():
+                stage_sum[k] = stage_sum.get(k, 0.0) + v
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    st = {k: round(v / args.steps, 3) for k, v in stage_sum.items()
+          if k in ("sy2sb", "bulge_chasing", "tridiagonal_dc", "total")}
+    st["tridiagonal_eigenvalues"] = st.pop("tridiagonal_dc")
+    line = {"metric": f"s per n={n} eigenvalues-only solve (FP64)", "value": ms / 1000.0,
+            "unit": "s/solve", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "dtype": "f64",
+            "data": "synthetic: seeded symmetrised Gaussian",
+            "config": {"workload": f"eigenvalues only n={n} b=32 nb={nb}"}, "stages_ms": st}
+    print(json.dumps(line))
+    return 0
+
+
 def run_serving(args) -> int:
     """Continuous-batching serving loop on a seeded Poisson stream."""
     import torch
@@ -409,7 +451,7 @@ def main(argv=None) -> int:
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--nb", type=int, default=1024)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU LAPACK baseline")
-    ap.add_argument("--workload", choices=("evd", "batched", "serving"), default="evd",
+    ap.add_argument("--workload", choices=("evd", "values", "batched", "serving"), default="evd",
                     help="evd (default): the n=16384 solve; batched / serving: the uneven-size "
                          "batch and the serving loop (one GPU)")
     ap.add_argument("--streams", type=int, default=8, help="worker streams (batched/serving)")
@@ -425,6 +467,8 @@ def main(argv=None) -> int:
         return run_batched(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "values":
+        return run_values(args)
     return run_ours(args)
 
 
