@@ -31,11 +31,12 @@
 // accumulator layout of an 8-row tile doubles as the A operand of the next
 // product (the k index is permuted to rows 0,2,4,6,1,3,5,7 and the B operand
 // is read with the same permutation), so the window is never shuffled.
-// T (Y^T Y by m8n8k4, then a triangular solve by 8 lanes) is either built by
-// a separate fully parallel kernel into a caller workspace before the apply
-// kernel runs (q2_tbuild_kernel; the apply kernel then stages it with the
-// reflectors), or, without a workspace, built inside the apply kernel one
-// block ahead.  U is staged by cp.async into zero-padded, bank-conflict-free
+// T (Y^T Y by m8n8k4, then a triangular solve by 8 lanes) is either built,
+// together with V = Y T^T (forward) or Y T (reverse), by a separate fully
+// parallel kernel into a caller workspace before the apply kernel runs
+// (q2_tbuild_kernel; the apply kernel then stages -V with the reflectors and
+// updates X^T += W (-V)^T, with no T product), or, without a workspace,
+// built inside the apply kernel one block ahead.  U is staged by cp.async into zero-padded, bank-conflict-free
 // segments three blocks deep.  Work: the
 // 2 n^2 ncols flops of the reflector algebra are done as 2.75 n^2 ncols on
 // the DMMA pipe (parallelogram padding 40/32, plus the T product), plus the
@@ -57,8 +58,10 @@ constexpr int kSeg = 64;                 // smem slots per (sweep, segment): 8 +
 constexpr int kYBuf = 8 * kGroups * kSeg;  // 8 sweeps x kGroups segments
 constexpr int kNYBuf = 3;
 constexpr int kTBuf = kGroups * 32 * 2;  // per group: 32 lanes x 2 B-fragment values
+constexpr int kVGroup = 5 * 32 * 2;      // per group: 5 tiles x 32 lanes x 2 B-fragment values
+constexpr int kVBuf = kGroups * kVGroup;
 constexpr int kGBuf = 64;                // per warp: one 8 x 8 Gram matrix
-constexpr size_t kQSmem = (size_t)(kNYBuf * kYBuf + kNYBuf * kTBuf + kQW * kGBuf) * sizeof(double);
+constexpr size_t kQSmem = (size_t)(kNYBuf * kYBuf + kNYBuf * kVBuf + kQW * kGBuf) * sizeof(double);
 static_assert(kGroups == kQW, "one warp builds the T of one group");
 
 __device__ __forceinline__ void cp_async8_zfill(double* smem, const double* gmem, bool valid) {
@@ -163,14 +166,72 @@ __device__ __forceinline__ void build_t(const double* ys, double* ts, double* gs
   }
 }
 
+// -V fragments of group w of a staged block (warp w), V = Y T^T (forward) or
+// Y T (reverse), so that the update X^T += W (-V)^T needs no T product:
+// lane (g, t) of tile i gets (-V[8i+g][2t], -V[8i+g][2t+1]).  T comes from
+// build_t's Gram/triangular solve (written to gs as T[i][q] at gs[i*8+q]).
+template <bool FWD>
+__device__ __forceinline__ void build_v(const double* ys, double* vs, double* gs, int warp,
+                                        int lane, int offW) {
+  const int j = warp;
+  {
+    double ga[2] = {0.0, 0.0}, gb[2] = {0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const double y0 = ys[offW + j * kSeg + 8 * i];
+      const double y1 = ys[offW + j * kSeg + 8 * i + 1];
+      mma8(ga, y0, y0);
+      mma8(gb, y1, y1);
+    }
+    const int g = lane >> 2, t = lane & 3;
+    gs[g * 8 + 2 * t] = ga[0] + gb[0];
+    gs[g * 8 + 2 * t + 1] = ga[1] + gb[1];
+  }
+  __syncwarp();
+  double tq[8];
+  if (lane < 8) {
+    const int q = lane;
+#pragma unroll
+    for (int i = 7; i >= 0; --i) {
+      double acc = 0.0;
+#pragma unroll
+      for (int k = i + 1; k < 8; ++k) acc = fma(gs[i * 8 + k], tq[k], acc);
+      tq[i] = (i < q) ? -acc : (i == q ? 1.0 : 0.0);
+    }
+  }
+  __syncwarp();
+  if (lane < 8) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) gs[i * 8 + lane] = tq[i];  // T[i][q]
+  }
+  __syncwarp();
+  const int g = lane >> 2, t = lane & 3;
+  double* dst = vs + j * kVGroup;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = 8 * i + g, p = 2 * t + h;
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double y = ys[seg_off(q, j) + r - q];  // zero outside the parallelogram
+        const double tv = FWD ? gs[p * 8 + q] : gs[q * 8 + p];
+        v = fma(y, tv, v);
+      }
+      dst[(i * 32 + lane) * 2 + h] = -v;
+    }
+  }
+}
+
 // Blocks of all strips, strip-major: strip s has nblk(s) = B0 - 16 s blocks
-// (B0 = ceil((n-2)/8); every strip height is a multiple of 8 rows), so the T
-// fragments of block bb of strip s start at tblock(s, bb) * kTBuf.
+// (B0 = ceil((n-2)/8); every strip height is a multiple of 8 rows), so the
+// precomputed fragments of block bb of strip s start at tblock(s, bb) * kVBuf.
 __host__ __device__ __forceinline__ long tblock(long s, long bb, long B0) {
   return s * B0 - 8 * s * (s - 1) + bb;
 }
 
-// -T fragments of every block of every strip (one CTA per block, one warp
+// -V fragments of every block of every strip (one CTA per block, one warp
 // per group), in the layout the apply kernel reads.
 template <bool FWD>
 __global__ void __launch_bounds__(kQThreads)
@@ -191,7 +252,7 @@ __global__ void __launch_bounds__(kQThreads)
   cp_commit();
   cp_wait<0>();
   __syncthreads();
-  build_t<FWD>(ys, Tg + tblock(s, bb, B0) * kTBuf, gsh + warp * kGBuf, warp, lane,
+  build_v<FWD>(ys, Tg + tblock(s, bb, B0) * kVBuf, gsh + warp * kGBuf, warp, lane,
                seg_off(g, 0) + 2 * t - g);
 }
 
@@ -218,7 +279,7 @@ __device__ __forceinline__ void w_part(const double (&x)[kTiles][4], const doubl
 // reverse: tile 4J+4 = the next group's first), so the next group's W over
 // its other four tiles is issued between this group's T product and its
 // update, and the shared tile is updated first.
-template <bool FWD>
+template <bool FWD, bool VPRE>
 __device__ __forceinline__ void apply_block(double (&x)[kTiles][4], const double* ys,
                                             const double* ts, int lane, int offW, int offU0,
                                             int offU1) {
@@ -231,16 +292,28 @@ __device__ __forceinline__ void apply_block(double (&x)[kTiles][4], const double
 #pragma unroll
     for (int q = 0; q < 4; ++q) wa[q] += wb[q];
     double wt[4] = {0.0, 0.0, 0.0, 0.0};
-    const double2 tf = *reinterpret_cast<const double2*>(ts + J * 64 + lane * 2);
-    mma16(wt, wa[0], wa[2], wa[1], wa[3], tf.x, tf.y);
+    if (VPRE) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) wt[q] = wa[q];  // the update reads -V instead of -T Y^T
+    } else {
+      const double2 tf = *reinterpret_cast<const double2*>(ts + J * 64 + lane * 2);
+      mma16(wt, wa[0], wa[2], wa[1], wa[3], tf.x, tf.y);
+    }
     double na[4] = {0.0, 0.0, 0.0, 0.0}, nb[4] = {0.0, 0.0, 0.0, 0.0};
     if (s + 1 < kGroups) w_part(x, ys, offW, JN, FWD ? 0 : 1, FWD ? 4 : 5, na, nb);
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       const int i = FWD ? k : 4 - k;  // shared tile first
       const int ti = 4 * J + i;
-      const double b0 = ys[offU0 + J * kSeg + 8 * i];
-      const double b1 = ys[offU1 + J * kSeg + 8 * i];
+      double b0, b1;
+      if (VPRE) {
+        const double2 vf = *reinterpret_cast<const double2*>(ts + J * kVGroup + (i * 32 + lane) * 2);
+        b0 = vf.x;
+        b1 = vf.y;
+      } else {
+        b0 = ys[offU0 + J * kSeg + 8 * i];
+        b1 = ys[offU1 + J * kSeg + 8 * i];
+      }
       mma16(x[ti], wt[0], wt[2], wt[1], wt[3], b0, b1);
     }
     if (s + 1 < kGroups) {
@@ -290,8 +363,8 @@ __global__ void __launch_bounds__(kQThreads, 2)
                   const double* __restrict__ Tg, double* __restrict__ X, long ldX) {
   extern __shared__ __align__(16) double smem[];
   double* Ys = smem;                 // kNYBuf x kYBuf
-  double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kTBuf (PRE) or 2 x kTBuf
-  double* Gs = Ts + kNYBuf * kTBuf;  // kQW x kGBuf
+  double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kVBuf (PRE: -V) or 2 x kTBuf (-T)
+  double* Gs = Ts + kNYBuf * kVBuf;  // kQW x kGBuf
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, t = lane & 3;
   double* gs = Gs + warp * kGBuf;
@@ -316,10 +389,10 @@ __global__ void __launch_bounds__(kQThreads, 2)
   double x[kTiles][4];
   const int nstrips = (n - 2 + kStrip - 1) / kStrip;
   const int B0 = (n - 2 + 7) / 8;
-  // stage the -T fragments of block bb of strip sidx (one 16-byte copy per thread)
+  // stage the -V fragments of block bb of strip sidx (16-byte copies)
   auto stage_t = [&](double* dst, int sidx, int bb) {
-    const double* src = Tg + tblock(sidx, bb, B0) * kTBuf;
-    for (int e = threadIdx.x; e < kTBuf / 2; e += kQThreads) cp_async16(dst + 2 * e, src + 2 * e);
+    const double* src = Tg + tblock(sidx, bb, B0) * kVBuf;
+    for (int e = threadIdx.x; e < kVBuf / 2; e += kQThreads) cp_async16(dst + 2 * e, src + 2 * e);
   };
   for (int si = 0; si < nstrips; ++si) {
     const int sidx = FWD ? (nstrips - 1 - si) : si;
@@ -339,7 +412,7 @@ __global__ void __launch_bounds__(kQThreads, 2)
     cp_commit();
     if (nblk > 1) {
       stage_block(Ys + kYBuf, U, ldU, n, R, H, bb_of(1));
-      if (PRE) stage_t(Ts + kTBuf, sidx, bb_of(1));
+      if (PRE) stage_t(Ts + kVBuf, sidx, bb_of(1));
     }
     cp_commit();
     cp_wait<1>();
@@ -354,17 +427,17 @@ __global__ void __launch_bounds__(kQThreads, 2)
       __syncthreads();  // block it+1 staged; T of block it complete
       if (it + 2 < nblk) {
         stage_block(Ys + ((it + 2) % 3) * kYBuf, U, ldU, n, R, H, bb_of(it + 2));
-        if (PRE) stage_t(Ts + ((it + 2) % 3) * kTBuf, sidx, bb_of(it + 2));
+        if (PRE) stage_t(Ts + ((it + 2) % 3) * kVBuf, sidx, bb_of(it + 2));
       }
       cp_commit();
       double inc[4];
       load_tile(inc, io, FWD ? (base + 8 * kTiles) : (base - 8), n);
       const double* ys = Ys + (it % 3) * kYBuf;
-      const double* ts = Ts + (PRE ? (it % 3) : (it & 1)) * kTBuf;
+      const double* ts = Ts + (PRE ? (it % 3) * kVBuf : (it & 1) * kTBuf);
       if (!PRE && it + 1 < nblk)
         build_t<FWD>(Ys + ((it + 1) % 3) * kYBuf, Ts + ((it + 1) & 1) * kTBuf, gs, warp, lane,
                      offW);
-      apply_block<FWD>(x, ys, ts, lane, offW, offU0, offU1);
+      apply_block<FWD, PRE>(x, ys, ts, lane, offW, offU0, offU1);
       // slide the window one tile: the tile leaving it is final for this strip
       if (FWD) {
         store_tile(x[0], io, base, n);
@@ -424,7 +497,7 @@ long q2_tbuf_doubles(long n) {
   if (n < 3) return 0;
   const long nstrips = (n - 2 + kStrip - 1) / kStrip;
   const long B0 = (n - 2 + 7) / 8;
-  return tblock(nstrips, 0, B0) * kTBuf;
+  return tblock(nstrips, 0, B0) * kVBuf;
 }
 
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,

@@ -168,11 +168,11 @@ __global__ void __launch_bounds__(kChaseThreads)
         const double nrm2 = warp_sum(x * x);
         double u = 0.0;
         if (nrm2 > 0.0) {
-          u = x * (1.0 / sqrt(nrm2));
+          u = x * rsqrt(nrm2);
           const double u0 = __shfl_sync(0xffffffffu, u, 0);
           const double u0n = u0 + ((u0 >= 0.0) ? 1.0 : -1.0);
           if (lane == 0) u = u0n;
-          u *= 1.0 / sqrt(fabs(u0n));
+          u *= rsqrt(fabs(u0n));
         }
         sm.u[lane] = u;
         if (U != nullptr && lane < rb) U[(r + lane) + (long)s * ldU] = u;

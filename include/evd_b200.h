@@ -181,9 +181,9 @@ int evd_bc_back(double* Q, long ldQ, const double* U, long ldU, long n, int b,
 /* X <- Q2 * X for an n x ncols block X (the eigenvector direction: reflectors
  * applied in reverse generation order; the reference applies Q2 through
  * my_SBRBack_BCBack, src/EVD/myEVD.cu:135-249).  `work` (16-byte aligned,
- * evd_bc_back_work_size(n) doubles, about n^2/8) receives the compact-WY
- * T factors of the reflector groups, built once for all columns; with
- * work == NULL they are rebuilt inside the apply kernel (slower). */
+ * evd_bc_back_work_size(n) doubles, about 5 n^2/8) receives the compact-WY
+ * factors V = Y T of the reflector groups, built once for all columns; with
+ * work == NULL the T factors are rebuilt inside the apply kernel (slower). */
 long evd_bc_back_work_size(long n);
 int evd_bc_back_apply(long n, long ncols, const double* U, long ldU, double* X, long ldX,
                       int b, double* work, long lwork, cudaStream_t stream);
