@@ -923,8 +923,11 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
       nrmax = std::max(nrmax, dd[D_NROT]);
     }
     a.Kmax = Kmax;
-    a.K12max = K12;
-    a.K23max = K23;
+    // leading dimensions of Qt/Ut and Qb/Ub rounded up to even: 16-byte
+    // aligned columns and batch strides keep the merge GEMMs on the lean
+    // kernel's 16-byte copies (the padding is zero-filled by gather/vectors)
+    a.K12max = (K12 + 1) & ~1;
+    a.K23max = (K23 + 1) & ~1;
     if (nrmax > 0) {
       merge_rotate_kernel<<<gN, 256, 0, st>>>(a);
       EVD_LAUNCHED();
@@ -948,12 +951,14 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
       // Zn[0:n1, 0:Kmax] = Qt Ut ; Zn[n1:N, 0:Kmax] = Qb Ub   (batched over merges)
       const long sZ = (long)a.N * a.N;
       if (K12 > 0) {
-        EVD_TRY(dgemm_batched('n', 'n', a.n1, Kmax, K12, 1.0, a.Qt, a.n1, (long)a.n1 * K12, a.Ut,
-                              K12, (long)K12 * Kmax, 0.0, a.Zn, a.N, sZ, a.nm, st));
+        EVD_TRY(dgemm_batched('n', 'n', a.n1, Kmax, K12, 1.0, a.Qt, a.n1, (long)a.n1 * a.K12max,
+                              a.Ut, a.K12max, (long)a.K12max * Kmax, 0.0, a.Zn, a.N, sZ, a.nm,
+                              st));
       }
       if (K23 > 0) {
-        EVD_TRY(dgemm_batched('n', 'n', a.n2, Kmax, K23, 1.0, a.Qb, a.n2, (long)a.n2 * K23, a.Ub,
-                              K23, (long)K23 * Kmax, 0.0, a.Zn + a.n1, a.N, sZ, a.nm, st));
+        EVD_TRY(dgemm_batched('n', 'n', a.n2, Kmax, K23, 1.0, a.Qb, a.n2, (long)a.n2 * a.K23max,
+                              a.Ub, a.K23max, (long)a.K23max * Kmax, 0.0, a.Zn + a.n1, a.N, sZ,
+                              a.nm, st));
       }
       if (K12 == 0 || K23 == 0) {
         // the missing half of the root columns is zero
