@@ -374,6 +374,18 @@ struct TileCopy {
                  bytes);
     }
   }
+  // Same with one precomputed pointer per strided line (the line's element
+  // ci of the tile is rows[r][koff]).
+  __device__ __forceinline__ void issue_rows(double* smem, const double* const (&rows)[R],
+                                             long koff, int cb, unsigned mk,
+                                             const double* safe) const {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int bytes = ((mk >> r) & 1u) ? cb : 0;
+      cp_async16(smem + (si0 + r * SS) * (CL + kPad) + ci, bytes ? rows[r] + koff : safe,
+                 bytes);
+    }
+  }
 };
 
 template <bool TA, bool TB, int BM, int BN, int BK, int WM, int WN, int STAGES, int MMA>
@@ -448,6 +460,17 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
   unsigned a_mk = ~0u, b_mk = ~0u;
   if (!TA) a_cb = ACopy::cbytes(p.m - m0 - ac.ci);
   else a_mk = ac.smask(p.m - m0);
+  // transposed A: rows m >= m1 of op(A) come from Am2 (the stacked operand of
+  // the ZY update); one pointer per copied line, fixed for the whole kernel
+  const double* arow[ACopy::R];
+  if (TA) {
+#pragma unroll
+    for (int r = 0; r < ACopy::R; ++r) {
+      const int mg = m0 + ac.si0 + r * ACopy::SS;
+      arow[r] = (mg < p.m1 || p.Am2 == nullptr) ? Ab + ac.ci + (long)mg * p.lda
+                                                : p.Am2 + ac.ci + (long)(mg - p.m1) * p.ldam2;
+    }
+  }
   if (TB) b_cb = BCopy::cbytes(p.n - n0 - bc.ci);
   else b_mk = bc.smask(p.n - n0);
 
@@ -465,9 +488,8 @@ __global__ void __launch_bounds__((BM / WM) * (BN / WN) * 32)
       const unsigned mk = (klim >= BK) ? ~0u : ac.smask(klim);
       ac.issue(as, g, (long)ACopy::SS * ld, a_cb, mk, p.A);
     } else {
-      const double* g = Ab + (long)(k0 + ac.ci) + (long)(m0 + ac.si0) * p.lda;
       const int cb = (klim >= BK) ? 16 : ACopy::cbytes(klim - ac.ci);
-      ac.issue(as, g, (long)ACopy::SS * p.lda, cb, a_mk, p.A);
+      ac.issue_rows(as, arow, k0, cb, a_mk, p.A);
     }
     if (!TB) {
       const double* g = Bb + (long)(k0 + bc.ci) + (long)(n0 + bc.si0) * p.ldb;
@@ -620,8 +642,8 @@ int dispatch_shape(GemmArgs p, long batch, cudaStream_t st) {
   // the skinny n = 32 ZY products run best as 64x32 tiles with split-K).
   // The lean kernel serves every call whose operands are 16-byte aligned and
   // whose K-split operand pair (if any) switches at a multiple of BK = 16;
-  // the general kernel covers the rest (M-split pairs, odd alignments).
-  const bool fast = p.vecA && p.vecB && (p.Am2 == nullptr || p.m1 >= p.m) &&
+  // the general kernel covers the rest (odd alignments).
+  const bool fast = p.vecA && p.vecB && (TA || p.Am2 == nullptr || p.m1 >= p.m) &&
                     (p.k1 >= p.k || p.k1 % 16 == 0);
   if (p.n <= 32 && p.mode == kGemm) {
     constexpr int BM = 64, BN = 32;
