@@ -86,8 +86,8 @@ thread_local double g_timings[6] = {0, 0, 0, 0, 0, 0};
 
 }  // namespace
 
-int syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X, long ldX,
-          void* work, long lwork_bytes, int timed, cudaStream_t st) {
+static int syevd_core(long n, long b, long nb, const double* A, long lda, double* w, double* X,
+                      long ldX, void* work, long lwork_bytes, int timed, cudaStream_t st) {
   if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
   long q = nb / b;
   if (q & (q - 1)) return EVD_ERR_INVALID_ARG;  // slab merge needs nb = b * 2^k
@@ -156,8 +156,8 @@ size_t syevd_ws_bytes(long n, long b, long nb) { return layout(n, b, nb).bytes; 
 // Eigenvalues only: stage 1, the chase without storing reflectors, and
 // Sturm-count multisection on the tridiagonal (no vectors, no back
 // transformation).  Same workspace as syevd.
-int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
-                 long lwork_bytes, int timed, cudaStream_t st) {
+static int values_core(long n, long b, long nb, const double* A, long lda, double* w,
+                       void* work, long lwork_bytes, int timed, cudaStream_t st) {
   if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
   if (lda < n || !A || !w || !work) return EVD_ERR_INVALID_ARG;
   SyevdLayout L = layout(n, b, nb);
@@ -202,9 +202,141 @@ int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, 
 
 }  // namespace evd
 
+namespace evd {
+namespace {
+
+// ---- any order n: padding to a multiple of nb ----
+// A of order n is embedded in A' = [A 0; 0 D] of order n' = nb * ceil(n / nb),
+// D = diag(2s + s k / (n'-n)), s >= ||A||_1 >= ||A||_2 (computed on the device).
+// A' is block diagonal, so its n smallest eigenvalues are A's, and the
+// leading n x n block of its eigenvectors holds A's eigenvectors.
+
+__global__ void col_abs_sum_kernel(long n, const double* __restrict__ A, long lda,
+                                   double* __restrict__ cs) {
+  __shared__ double red[32];
+  const long j = blockIdx.x;
+  double acc = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) acc += fabs(A[i + j * lda]);
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+    cs[j] = t;
+  }
+}
+
+__global__ void pad_fill_kernel(long n, long np, const double* __restrict__ cs,
+                                double* __restrict__ Ap, long ldp) {
+  // s = max column sum (every block recomputes it: n <= a few 10^5 reads)
+  __shared__ double red[32];
+  double m = 0.0;
+  for (long j = threadIdx.x; j < n; j += blockDim.x) m = fmax(m, cs[j]);
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  double sv = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) sv = fmax(sv, red[k]);
+  if (!(sv > 0.0)) sv = 1.0;  // zero matrix: pad values 2 .. 3 sit above its eigenvalues
+  const long kpad = np - n;
+  // column c of A' outside A's block: zero, with the pad value on the diagonal;
+  // rows n.. of A's columns: zero
+  for (long c = blockIdx.x; c < np; c += gridDim.x) {
+    if (c < n) {
+      for (long i = n + threadIdx.x; i < np; i += blockDim.x) Ap[i + c * ldp] = 0.0;
+    } else {
+      const double dv = 2.0 * sv + sv * (double)(c - n) / (double)kpad;
+      for (long i = threadIdx.x; i < np; i += blockDim.x) Ap[i + c * ldp] = (i == c) ? dv : 0.0;
+    }
+  }
+}
+
+// at least 64 (two b = 32 panels), so the smallest problems take the same path
+long padded_order(long n, long nb) { return std::max<long>((n + nb - 1) / nb * nb, 64); }
+bool needs_pad(long n, long nb) { return n % nb != 0 || n < 64; }
+
+struct PadLayout {
+  long np;
+  size_t core_bytes, oAp, oXp, owp, ocs, bytes;  // offsets in doubles after the core part
+};
+
+PadLayout pad_layout(long n, long b, long nb) {
+  PadLayout P{};
+  P.np = padded_order(n, nb);
+  P.core_bytes = syevd_ws_bytes(P.np, b, nb);
+  const size_t base = (P.core_bytes + 255) / 8 + 32;  // doubles, past the core region
+  auto al = [](size_t x) { return (x + 31) / 32 * 32; };
+  size_t o = al(base);
+  P.oAp = o; o = al(o + (size_t)P.np * P.np);
+  P.oXp = o; o = al(o + (size_t)P.np * P.np);
+  P.owp = o; o = al(o + P.np);
+  P.ocs = o; o = al(o + n);
+  P.bytes = o * sizeof(double) + 256;
+  return P;
+}
+
+int pad_prepare(long n, const double* A, long lda, const PadLayout& P, double* base,
+                cudaStream_t st) {
+  double* Ap = base + P.oAp;
+  double* cs = base + P.ocs;
+  col_abs_sum_kernel<<<(unsigned)n, 256, 0, st>>>(n, A, lda, cs);
+  EVD_LAUNCHED();
+  EVD_TRY(copy_matrix(n, n, A, lda, Ap, P.np, st));
+  pad_fill_kernel<<<(unsigned)std::min<long>(P.np, 4096), 256, 0, st>>>(n, P.np, cs, Ap, P.np);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+bool shape_ok(long n, long b, long nb) {
+  return n > 0 && b == 32 && nb > 0 && nb % b == 0 && ((nb / b) & (nb / b - 1)) == 0;
+}
+
+}  // namespace
+
+size_t syevd_any_ws_bytes(long n, long b, long nb) {
+  if (!needs_pad(n, nb)) return syevd_ws_bytes(n, b, nb);
+  return pad_layout(n, b, nb).bytes;
+}
+
+int syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X, long ldX,
+          void* work, long lwork_bytes, int timed, cudaStream_t st) {
+  if (!shape_ok(n, b, nb)) return EVD_ERR_INVALID_ARG;
+  if (!needs_pad(n, nb)) return syevd_core(n, b, nb, A, lda, w, X, ldX, work, lwork_bytes, timed, st);
+  if (lda < n || ldX < n || !A || !w || !X || !work) return EVD_ERR_INVALID_ARG;
+  const PadLayout P = pad_layout(n, b, nb);
+  if ((size_t)lwork_bytes < P.bytes) return EVD_ERR_WORKSPACE;
+  double* base = reinterpret_cast<double*>(work);
+  EVD_TRY(pad_prepare(n, A, lda, P, base, st));
+  EVD_TRY(syevd_core(P.np, b, nb, base + P.oAp, P.np, base + P.owp, base + P.oXp, P.np, work,
+                     (long)P.core_bytes, timed, st));
+  EVD_CUDA_TRY(cudaMemcpyAsync(w, base + P.owp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  EVD_TRY(copy_matrix(n, n, base + P.oXp, P.np, X, ldX, st));
+  EVD_CUDA_TRY(cudaStreamSynchronize(st));
+  return EVD_SUCCESS;
+}
+
+int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
+                 long lwork_bytes, int timed, cudaStream_t st) {
+  if (!shape_ok(n, b, nb)) return EVD_ERR_INVALID_ARG;
+  if (!needs_pad(n, nb)) return values_core(n, b, nb, A, lda, w, work, lwork_bytes, timed, st);
+  if (lda < n || !A || !w || !work) return EVD_ERR_INVALID_ARG;
+  const PadLayout P = pad_layout(n, b, nb);
+  if ((size_t)lwork_bytes < P.bytes) return EVD_ERR_WORKSPACE;
+  double* base = reinterpret_cast<double*>(work);
+  EVD_TRY(pad_prepare(n, A, lda, P, base, st));
+  EVD_TRY(values_core(P.np, b, nb, base + P.oAp, P.np, base + P.owp, work, (long)P.core_bytes,
+                      timed, st));
+  EVD_CUDA_TRY(cudaMemcpyAsync(w, base + P.owp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  EVD_CUDA_TRY(cudaStreamSynchronize(st));
+  return EVD_SUCCESS;
+}
+
+}  // namespace evd
+
 extern "C" long evd_syevd_work_size(long n, long b, long nb) {
-  if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return 0;
-  return (long)evd::syevd_ws_bytes(n, b, nb);
+  if (!evd::shape_ok(n, b, nb)) return 0;
+  return (long)evd::syevd_any_ws_bytes(n, b, nb);
 }
 
 extern "C" void evd_syevd_last_timings(double out_ms[6]) {

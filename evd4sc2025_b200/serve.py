@@ -4,12 +4,11 @@ Both sit on the plain FP64 solver (``evd_syevd``).  The reference solves one
 matrix per process (``myEVD n b nb``, src/EVD/myEVD.cu:251-706, n a multiple
 of 1024); this layer adds:
 
-* **any n >= 1**: a matrix whose order is not a multiple of 32 is padded to
-  n' = 32 * ceil(n / 32) (at least 64) with a diagonal block placed above the
-  spectrum of A (values 2 s, 2 s + s/k, ... with s >= ||A||_2).  The padded
-  matrix is block diagonal, so its n smallest eigenvalues are those of A and
-  the leading n x n block of the eigenvectors holds A's eigenvectors;
-  nb = 32 * 2^k is the largest such divisor of n' up to 1024.
+* **any n >= 1** through ``evd_syevd`` itself, which pads an order that is
+  not a multiple of nb (or below 64) with a diagonal block above the
+  spectrum, on the device; nb = 32 * 2^k is chosen here as the largest one
+  dividing n' = 32 * ceil(n / 32) (n' >= 64), at most 1024, so the padded
+  order is n'.
 * **overlap on the device**: a pool of workers, each with its own CUDA
   stream, one grow-only workspace and padded buffer pair, and a host thread
   (the solver synchronises its own stream a few times per solve; ctypes
@@ -56,16 +55,17 @@ def padded_shape(n: int) -> tuple[int, int]:
 
 
 def footprint_bytes(n: int) -> int:
-    """Device bytes one solve of order n holds: workspace + padded A and X + w."""
-    np_, nb = padded_shape(n)
-    return int(lib().evd_syevd_work_size(np_, 32, nb)) + 2 * np_ * np_ * 8 + np_ * 8
+    """Device bytes one solve of order n holds: workspace (with the padded
+    copies when n' > n) + A and X of order n + w."""
+    _, nb = padded_shape(n)
+    return int(lib().evd_syevd_work_size(n, 32, nb)) + 2 * n * n * 8 + n * 8
 
 
 class StreamSolver:
     """One worker: a CUDA stream, one grow-only workspace and one pair of
-    padded A/X buffers (a smaller problem uses the leading block of the
-    buffers, with their leading dimension), so a worker holds at most the
-    footprint of the largest problem it has solved."""
+    A/X buffers (a smaller problem uses the leading block of the buffers,
+    with their leading dimension), so a worker holds at most the footprint
+    of the largest problem it has solved."""
 
     def __init__(self, device="cuda"):
         self.device = torch.device(device)
@@ -75,21 +75,21 @@ class StreamSolver:
         self._ld = 0
         self._A = self._X = self._w = None
 
-    def _ensure(self, np_: int, nb: int):
-        need = int(lib().evd_syevd_work_size(np_, 32, nb))
+    def _ensure(self, n: int, nb: int):
+        need = int(lib().evd_syevd_work_size(n, 32, nb))
         if need <= 0:
-            raise ValueError(f"unsupported padded order {np_} (nb {nb})")
+            raise ValueError(f"unsupported order {n} (nb {nb})")
         if need > self._wsbytes:
             self._ws = None
             self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
             self._wsbytes = need
-        if np_ > self._ld:
+        if n > self._ld:
             self._A = self._X = self._w = None
-            self._A = empty_cm(np_, np_, device=self.device)
-            self._X = empty_cm(np_, np_, device=self.device)
-            self._w = torch.empty(np_, dtype=F64, device=self.device)
-            self._ld = np_
-        return self._A[:np_, :np_], self._X[:np_, :np_], self._w[:np_]
+            self._A = empty_cm(n, n, device=self.device)
+            self._X = empty_cm(n, n, device=self.device)
+            self._w = torch.empty(n, dtype=F64, device=self.device)
+            self._ld = n
+        return self._A[:n, :n], self._X[:n, :n], self._w[:n]
 
     def release(self):
         """Drop the workspace and buffers (their memory returns to torch)."""
@@ -99,26 +99,20 @@ class StreamSolver:
     def solve(self, A: torch.Tensor):
         """Eigenvalues (ascending, length n) and eigenvectors (n x n,
         column-major) of the symmetric FP64 matrix A on this worker's stream.
-        A may live on the host or the device; results are on the device."""
+        A may live on the host or the device; results are on the device.
+        Nothing here synchronises the host: the padding runs on the device."""
         n = A.shape[0]
-        np_, nb = padded_shape(n)
+        _, nb = padded_shape(n)
         with torch.cuda.stream(self.stream):
-            Ap, Xp, wp = self._ensure(np_, nb)
-            Ap.zero_()
-            Ap[:n, :n].copy_(A, non_blocking=True)
-            if np_ > n:
-                s = float(torch.linalg.matrix_norm(Ap[:n, :n], ord=1))
-                s = max(s, 1e-300)
-                k = np_ - n
-                pad = 2.0 * s + s * torch.arange(k, dtype=F64, device=self.device) / k
-                Ap[n:, n:].diagonal().copy_(pad)
-            pa, lda = _cm(Ap, "A")
-            px, ldx = _cm(Xp, "X")
-            call("evd_syevd", np_, 32, nb, pa, lda, _ptr(wp), px, ldx, _ptr(self._ws),
+            Ab, Xb, wb = self._ensure(n, nb)
+            Ab.copy_(A, non_blocking=True)
+            pa, lda = _cm(Ab, "A")
+            px, ldx = _cm(Xb, "X")
+            call("evd_syevd", n, 32, nb, pa, lda, _ptr(wb), px, ldx, _ptr(self._ws),
                  self._wsbytes, 0, _stream(self.stream))
-            w = wp[:n].clone()
+            w = wb.clone()
             X = empty_cm(n, n, device=self.device)
-            X.copy_(Xp[:n, :n])
+            X.copy_(Xb)
         return w, X
 
 

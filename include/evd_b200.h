@@ -230,7 +230,9 @@ int evd_check_eig(long n, const double* A, long lda, const double* w, const doub
 
 /* ---- Whole solver ------------------------------------------------------- */
 
-/* Bytes of device workspace for evd_syevd. */
+/* Bytes of device workspace for evd_syevd and evd_syevd_values (0 for an
+ * unsupported shape: b != 32, nb not 32 * 2^k, n < 1).  Any n >= 1 is accepted;
+ * when n % nb != 0 the workspace also holds the padded copies (see evd_syevd). */
 long evd_syevd_work_size(long n, long b, long nb);
 
 /* Stage timings (milliseconds, CUDA events) of the last evd_syevd call on this
@@ -242,7 +244,12 @@ void evd_syevd_last_timings(double out_ms[6]);
  * symmetric A (device, full storage; A is not modified).  The plain-FP64
  * two-stage pipeline of the reference driver `myEVD n b nb`
  * (src/EVD/myEVD.cu:251-706): sy2sb -> bulge chasing -> tridiagonal D&C ->
- * stage-2 then stage-1 back transformation.  work: evd_syevd_work_size bytes. */
+ * stage-2 then stage-1 back transformation.  work: evd_syevd_work_size bytes.
+ * The reference requires n % nb == 0; here any n >= 1 is accepted: A is embedded
+ * in A' = [A 0; 0 D] of order n' = nb * ceil(n / nb), D = diag(2s + s k / (n' - n)),
+ * s = ||A||_1 computed on the device (no host synchronisation), so A's
+ * eigenvalues are the n smallest of A' and the leading n x n block of A''s
+ * eigenvectors holds A's.  Stage timings then refer to the order-n' solve. */
 int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, double* X,
               long ldX, void* work, long lwork_bytes, int timed, cudaStream_t stream);
 
@@ -251,7 +258,7 @@ int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, dou
  * reference driver has no such mode (its eigenvalues come from the full
  * dstedc at src/EVD/myEVD.cu:465-491).  work: evd_syevd_work_size bytes;
  * evd_syevd_last_timings gives [0] sy2sb, [1] chasing, [2] tridiagonal
- * eigenvalues, [5] total. */
+ * eigenvalues, [5] total.  Any n >= 1, padded as in evd_syevd. */
 int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
                      long lwork_bytes, int timed, cudaStream_t stream);
 

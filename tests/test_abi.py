@@ -47,7 +47,10 @@ def test_workspace_queries(evdlib):
     assert lib.evd_sy2sb_work_size(4096, 32, 1024) > 0
     assert lib.evd_sy2sb_work_size(4096, 16, 1024) == 0  # b must be 32
     assert lib.evd_syevd_work_size(4096, 32, 1024) > 8 * 4096 * 4096 * 5
-    assert lib.evd_syevd_work_size(4000, 32, 1024) == 0  # n % nb != 0
+    # n % nb != 0: padded internally to 4096, workspace holds the padded copies
+    assert lib.evd_syevd_work_size(4000, 32, 1024) > lib.evd_syevd_work_size(4096, 32, 1024)
+    assert lib.evd_syevd_work_size(4096, 32, 96) == 0    # nb must be 32 * 2^k
+    assert lib.evd_syevd_work_size(0, 32, 64) == 0
     assert lib.evd_stedc_work_size(1000) > 1000 * 1000
     assert lib.evd_bulge_chase_iwork_size(1000) >= 4 * 1000
 

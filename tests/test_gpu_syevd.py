@@ -93,3 +93,43 @@ def test_structured_inputs(cuda, evdlib, kind):
     w_ref = np.linalg.eigvalsh(A)
     assert np.abs(w.cpu().numpy() - w_ref).max() <= 1e-12 * np.abs(A).max() * 8
     assert res <= 1e-13 and orth <= 1e-13, (res, orth)
+
+
+@pytest.mark.parametrize("n,nb", [(1000, 256), (300, 128), (1, 64), (20, 32), (32, 32),
+                                  (33, 32), (77, 64), (1500, 1024)])
+def test_syevd_any_order(cuda, evdlib, n, nb):
+    """n not a multiple of nb: padded internally with a decoupled diagonal
+    block above the spectrum; results must meet the same bars as n % nb == 0."""
+    A = O.sym_gaussian(n, seed=3 * n + 1)
+    w, X, res, orth = _run(cuda, evdlib, A, nb)
+    assert w.shape == (n,) and X.shape == (n, n)
+    w_ref = np.linalg.eigvalsh(A)
+    nA = max(np.linalg.norm(A, 2), 1e-300)
+    assert np.abs(w - w_ref).max() <= TOL_VAL * nA
+    assert res <= TOL_RES and orth <= TOL_ORT, (res, orth)
+    assert O.residual(A, w, X) <= TOL_RES
+
+
+def test_syevd_any_order_zero_and_strided(cuda, evdlib):
+    """A zero matrix (pad values fall back to 2 .. 3) and a strided A/X
+    (lda, ldX > n) in the padded path; A is not modified."""
+    n, nb = 200, 64
+    Zd = evdlib.to_cm(torch.zeros(n, n, dtype=torch.float64), device=cuda)
+    w, X = evdlib.syevd(Zd, 32, nb)
+    torch.cuda.synchronize()
+    Xh = X.cpu().numpy()
+    assert np.all(w.cpu().numpy() == 0.0)
+    assert np.linalg.norm(Xh.T @ Xh - np.eye(n)) / n <= TOL_ORT
+    A = O.sym_gaussian(n, seed=9)
+    big = evdlib.to_cm(torch.zeros(n + 7, n + 7, dtype=torch.float64), device=cuda)
+    big[:n, :n].copy_(torch.from_numpy(A))
+    Ad = big[:n, :n]
+    Xbig = evdlib.to_cm(torch.zeros(n + 5, n + 5, dtype=torch.float64), device=cuda)
+    Xd = Xbig[:n, :n]
+    before = Ad.clone()
+    w, X = evdlib.syevd(Ad, 32, nb, X=Xd)
+    torch.cuda.synchronize()
+    assert torch.equal(Ad, before)
+    assert np.abs(w.cpu().numpy() - np.linalg.eigvalsh(A)).max() <= TOL_VAL * np.linalg.norm(A, 2)
+    assert O.residual(A, w.cpu().numpy(), Xd.cpu().numpy()) <= TOL_RES
+    assert float(Xbig[n:, :].abs().max()) == 0.0  # rows past n of X untouched

@@ -77,3 +77,14 @@ def test_values_only_known_spectrum(cuda, evdlib, kind):
     w = evdlib.syevd_values(Ad, 32, 256)
     torch.cuda.synchronize()
     assert np.abs(w.cpu().numpy() - np.sort(lam)).max() <= 1e-12 * np.abs(lam).max() * 8
+
+
+@pytest.mark.parametrize("n,nb", [(1000, 256), (77, 64), (1, 64)])
+def test_values_only_any_order(cuda, evdlib, n, nb):
+    A = O.sym_gaussian(n, n + 11)
+    Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
+    w = evdlib.syevd_values(Ad, 32, nb)
+    torch.cuda.synchronize()
+    assert w.shape == (n,)
+    ref = np.linalg.eigvalsh(A)
+    assert np.abs(w.cpu().numpy() - ref).max() <= 1e-12 * max(np.linalg.norm(A, 2), 1e-300)
