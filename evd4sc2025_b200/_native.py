@@ -55,6 +55,14 @@ SIGNATURES = {
     "evd_stebz": (_i, [_l, _p, _p, _p, _p, _l, _p]),
     "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
+    "evd_write_matrix_bin": (_i, [C.c_char_p, _i, _l, _l, _p, _l]),
+    "evd_matrix_bin_count": (_l, [C.c_char_p]),
+    "evd_matrix_bin_shape": (_i, [C.c_char_p, _l, C.POINTER(_l), C.POINTER(_l)]),
+    "evd_read_matrix_bin": (_i, [C.c_char_p, _l, _l, _l, _p, _l]),
+    "evd_write_eigenpairs_bin": (_i, [C.c_char_p, _l, _p, _p, _l]),
+    "evd_read_eigenpairs_bin": (_i, [C.c_char_p, _l, _p, _p, _l]),
+    "evd_write_matrix_csv": (_i, [C.c_char_p, _l, _l, _p, _l]),
+    "evd_read_matrix_csv": (_i, [C.c_char_p, C.POINTER(_l), C.POINTER(_l), _p, _l]),
 }
 
 _LIB = None

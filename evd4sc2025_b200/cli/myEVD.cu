@@ -1,4 +1,5 @@
 // myEVD <n> <b> <nb> [--dist uniform|gauss] [--seed S] [--reps R] [--no-check]
+//       [--input A.bin] [--save-input A.bin] [--output eig.bin]
 //
 // Command-line driver with the reference's surface (src/EVD/myEVD.cu:251-266:
 // three positional arguments; a wrong count prints the usage and returns 0).
@@ -6,7 +7,9 @@
 // triangle mirrored to the upper one, the reference's input shape; --dist gauss
 // gives (G + G^T)/2), runs the B200 eigensolver through the C ABI, and prints
 // the stage times, the FP64 rate of each stage with its own flop count, and
-// the orthogonality / residual of the result.
+// the orthogonality / residual of the result.  --input reads A (n x n) from
+// record 0 of a binary matrix file instead; --save-input writes the generated
+// A; --output writes the eigenpairs (w, X) as a binary eigenpair file.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -62,16 +65,20 @@ int main(int argc, char** argv) {
   long n = atol(argv[1]), b = atol(argv[2]), nb = atol(argv[3]);
   int gauss = 0, reps = 1, check = 1;
   uint64_t seed = 3000;
+  const char *in_path = nullptr, *save_path = nullptr, *out_path = nullptr;
   for (int i = 4; i < argc; ++i) {
     if (!strcmp(argv[i], "--dist") && i + 1 < argc) gauss = !strcmp(argv[++i], "gauss");
     else if (!strcmp(argv[i], "--seed") && i + 1 < argc) seed = strtoull(argv[++i], 0, 10);
     else if (!strcmp(argv[i], "--reps") && i + 1 < argc) reps = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--no-check")) check = 0;
+    else if (!strcmp(argv[i], "--input") && i + 1 < argc) in_path = argv[++i];
+    else if (!strcmp(argv[i], "--save-input") && i + 1 < argc) save_path = argv[++i];
+    else if (!strcmp(argv[i], "--output") && i + 1 < argc) out_path = argv[++i];
   }
   printf("%s\nn=%ld, b=%ld, nb=%ld\n", evd_version(), n, b, nb);
   long wbytes = evd_syevd_work_size(n, b, nb);
   if (wbytes <= 0) {
-    printf("unsupported sizes: need b == 32, n %% nb == 0, nb = 32 * 2^k\n");
+    printf("unsupported sizes: need n >= 1, b == 32, nb = 32 * 2^k\n");
     return 1;
   }
   double *A, *w, *X;
@@ -80,9 +87,28 @@ int main(int argc, char** argv) {
   CK(cudaMalloc(&X, sizeof(double) * n * n));
   CK(cudaMalloc(&w, sizeof(double) * n));
   CK(cudaMalloc(&work, wbytes));
-  gen_sym<<<dim3((unsigned)((n + 255) / 256), (unsigned)n), 256>>>(n, A, n, seed, gauss);
-  CK(cudaGetLastError());
-  CK(cudaDeviceSynchronize());
+  if (in_path) {
+    long r = 0, c = 0;
+    int rc = evd_matrix_bin_shape(in_path, 0, &r, &c);
+    if (rc == EVD_SUCCESS && (r != n || c != n)) rc = EVD_ERR_INVALID_ARG;
+    if (rc == EVD_SUCCESS) rc = evd_read_matrix_bin(in_path, 0, n, n, A, n);
+    if (rc != EVD_SUCCESS) {
+      printf("cannot read a %ld x %ld matrix from %s: %s\n", n, n, in_path, evd_status_string(rc));
+      return 1;
+    }
+    printf("A read from %s\n", in_path);
+  } else {
+    gen_sym<<<dim3((unsigned)((n + 255) / 256), (unsigned)n), 256>>>(n, A, n, seed, gauss);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    if (save_path) {
+      int rc = evd_write_matrix_bin(save_path, 0, n, n, A, n);
+      if (rc != EVD_SUCCESS) {
+        printf("cannot write %s: %s\n", save_path, evd_status_string(rc));
+        return 1;
+      }
+    }
+  }
   double t[6];
   for (int r = 0; r < reps; ++r) {
     int rc = evd_syevd(n, b, nb, A, n, w, X, n, work, wbytes, 1, 0);
@@ -101,6 +127,14 @@ int main(int argc, char** argv) {
     printf("SBR back %ldx%ld takes %.3f ms, tflops is %.3f\n", n, n, t[4], 2.0 * n3 / (t[4] * 1e9));
     printf("total EVD %ldx%ld takes %.3f ms, FP64-equivalent tflops is %.3f\n", n, n, t[5],
            16.0 / 3.0 * n3 / (t[5] * 1e9));
+  }
+  if (out_path) {
+    int rc = evd_write_eigenpairs_bin(out_path, n, w, X, n);
+    if (rc != EVD_SUCCESS) {
+      printf("cannot write %s: %s\n", out_path, evd_status_string(rc));
+      return 1;
+    }
+    printf("eigenpairs written to %s\n", out_path);
   }
   if (check) {
     double* cw;

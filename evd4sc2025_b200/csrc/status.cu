@@ -9,6 +9,7 @@ extern "C" const char* evd_status_string(int status) {
     case EVD_ERR_TIMEOUT: return "bounded device wait timed out";
     case EVD_ERR_NO_CONVERGENCE: return "iteration did not converge";
     case EVD_ERR_WORKSPACE: return "workspace too small";
+    case EVD_ERR_IO: return "file I/O error";
     default: return "unknown status";
   }
 }

@@ -29,6 +29,7 @@ extern "C" {
 #define EVD_ERR_TIMEOUT (-3)       /* a bounded device-side wait ran out          */
 #define EVD_ERR_NO_CONVERGENCE (-4)/* an iterative solver did not converge        */
 #define EVD_ERR_WORKSPACE (-5)     /* workspace smaller than the size query says  */
+#define EVD_ERR_IO (-6)            /* a file could not be opened, read or written */
 
 /* Human-readable text for a status code (static storage). */
 const char* evd_status_string(int status);
@@ -261,6 +262,32 @@ int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, dou
  * eigenvalues, [5] total.  Any n >= 1, padded as in evd_syevd. */
 int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
                      long lwork_bytes, int timed, cudaStream_t stream);
+
+/* ---- Matrix and eigenpair files ----------------------------------------- */
+
+/* The reference has CSV only (writeMatrixToCsvV2, util/inc/fileOpTool.h:51-80;
+ * readMatrixFromFile + fillMatrix, util/tool/fileOpTool.cu:127-174).  Binary
+ * files here are a sequence of records: a 32-byte little-endian header
+ * {"EVDM", u32 version = 1, u32 elem_bytes = 8, u32 0, i64 rows, i64 cols}
+ * then rows * cols FP64 values, column-major.  Matrix pointers may be device
+ * or host memory.  Errors: EVD_ERR_IO (open/read/write failure, bad header,
+ * missing record), EVD_ERR_INVALID_ARG (bad size, or a shape that does not
+ * match the record). */
+int evd_write_matrix_bin(const char* path, int append, long rows, long cols, const double* A,
+                         long ldA);
+/* Number of records in the file (negative status on error). */
+long evd_matrix_bin_count(const char* path);
+int evd_matrix_bin_shape(const char* path, long index, long* rows, long* cols);
+int evd_read_matrix_bin(const char* path, long index, long rows, long cols, double* A, long ldA);
+/* Eigenpair file: record 0 = w (n x 1), record 1 = X (n x n). */
+int evd_write_eigenpairs_bin(const char* path, long n, const double* w, const double* X,
+                             long ldX);
+int evd_read_eigenpairs_bin(const char* path, long n, double* w, double* X, long ldX);
+/* CSV in the reference's layout (one matrix row per line, comma separated,
+ * %.17g).  evd_read_matrix_csv with A == NULL returns the shape in *rows,
+ * *cols; with A it checks the shape and reads. */
+int evd_write_matrix_csv(const char* path, long rows, long cols, const double* A, long ldA);
+int evd_read_matrix_csv(const char* path, long* rows, long* cols, double* A, long ldA);
 
 #ifdef __cplusplus
 }
