@@ -355,10 +355,12 @@ def run_batched(args) -> int:
             G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
             mats.append(0.5 * (G + G.t()))
         solvers = [serve.StreamSolver(dev) for _ in range(args.streams)]
-        serve.syevd_batched(mats[: 2 * args.streams], solvers=solvers)  # warm-up
+        # warm-up: one full pass, so the grow-only workspaces and the caching
+        # allocator have reached their size before the timed pass
+        serve.syevd_batched(mats, solvers=solvers)
         _, ms = serve.syevd_batched(mats, solvers=solvers)
         one = [serve.StreamSolver(dev)]
-        serve.syevd_batched(mats[:4], solvers=one)
+        serve.syevd_batched(sorted(mats, key=lambda m: -m.shape[0])[:4], solvers=one)
         _, ms_loop = serve.syevd_batched(mats, solvers=one)
         flops = sum(16.0 / 3.0 * n ** 3 for n in sizes)
         out.append({"batch": tag, "matrices": count, "n_range": [lo, hi],
@@ -368,7 +370,11 @@ def run_batched(args) -> int:
     line = {"metric": "batched solves/s (uneven sizes, FP64 accuracy)", "value": out[0]["solves_per_s"],
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
             "data": "synthetic: seeded symmetrised Gaussian, n log-uniform",
-            "config": {"workload": "batched uneven sizes", "streams": args.streams}, "batches": out}
+            "config": {"workload": "batched uneven sizes", "streams": args.streams,
+                       "nb": "fixed rule" if args.nb_rule or not serve.autotune.active_table()
+                       or not serve.autotune.active_table().get("entries") else
+                       "tuned table " + str(serve.autotune.DEFAULT_TABLE.name)},
+            "batches": out}
     print(json.dumps(line))
     return 0
 
@@ -457,6 +463,8 @@ def main(argv=None) -> int:
                     help="evd (default): the n=16384 solve; batched / serving: the uneven-size "
                          "batch and the serving loop (one GPU)")
     ap.add_argument("--streams", type=int, default=8, help="worker streams (batched/serving)")
+    ap.add_argument("--nb-rule", action="store_true",
+                    help="batched/serving: nb by the fixed rule instead of the tuned table")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--requests", type=int, default=1000)
     ap.add_argument("--rate", type=float, default=12.0, help="serving arrivals per second")
@@ -465,6 +473,9 @@ def main(argv=None) -> int:
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.nb_rule:  # batched / serving: the fixed nb rule instead of the tuned table
+        from evd4sc2025_b200 import autotune
+        autotune.use_table(None)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "serving":

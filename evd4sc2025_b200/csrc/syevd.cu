@@ -86,8 +86,11 @@ thread_local double g_timings[6] = {0, 0, 0, 0, 0, 0};
 
 }  // namespace
 
+// err_out != nullptr: the chase's error word is not read here; its address is
+// returned so the caller can enqueue more work before the one host read.
 static int syevd_core(long n, long b, long nb, const double* A, long lda, double* w, double* X,
-                      long ldX, void* work, long lwork_bytes, int timed, cudaStream_t st) {
+                      long ldX, void* work, long lwork_bytes, int timed, cudaStream_t st,
+                      const int** err_out = nullptr) {
   if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
   long q = nb / b;
   if (q & (q - 1)) return EVD_ERR_INVALID_ARG;  // slab merge needs nb = b * 2^k
@@ -148,6 +151,10 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
     for (auto& x : ev) cudaEventDestroy(x);
   }
   // chasing error word (bounded waits) is checked once at the end
+  if (err_out) {
+    *err_out = ich + n + 32;
+    return EVD_SUCCESS;
+  }
   return read_device_error(ich + n + 32, st);
 }
 
@@ -157,7 +164,8 @@ size_t syevd_ws_bytes(long n, long b, long nb) { return layout(n, b, nb).bytes; 
 // Sturm-count multisection on the tridiagonal (no vectors, no back
 // transformation).  Same workspace as syevd.
 static int values_core(long n, long b, long nb, const double* A, long lda, double* w,
-                       void* work, long lwork_bytes, int timed, cudaStream_t st) {
+                       void* work, long lwork_bytes, int timed, cudaStream_t st,
+                       const int** err_out = nullptr) {
   if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
   if (lda < n || !A || !w || !work) return EVD_ERR_INVALID_ARG;
   SyevdLayout L = layout(n, b, nb);
@@ -196,6 +204,10 @@ static int values_core(long n, long b, long nb, const double* A, long lda, doubl
     EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[3]));
     g_timings[5] = ms;
     for (auto& x : ev) cudaEventDestroy(x);
+  }
+  if (err_out) {
+    *err_out = ich + n + 32;
+    return EVD_SUCCESS;
   }
   return read_device_error(ich + n + 32, st);
 }
@@ -308,12 +320,12 @@ int syevd(long n, long b, long nb, const double* A, long lda, double* w, double*
   if ((size_t)lwork_bytes < P.bytes) return EVD_ERR_WORKSPACE;
   double* base = reinterpret_cast<double*>(work);
   EVD_TRY(pad_prepare(n, A, lda, P, base, st));
+  const int* err = nullptr;
   EVD_TRY(syevd_core(P.np, b, nb, base + P.oAp, P.np, base + P.owp, base + P.oXp, P.np, work,
-                     (long)P.core_bytes, timed, st));
+                     (long)P.core_bytes, timed, st, &err));
   EVD_CUDA_TRY(cudaMemcpyAsync(w, base + P.owp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   EVD_TRY(copy_matrix(n, n, base + P.oXp, P.np, X, ldX, st));
-  EVD_CUDA_TRY(cudaStreamSynchronize(st));
-  return EVD_SUCCESS;
+  return read_device_error(err, st);
 }
 
 int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
@@ -325,11 +337,11 @@ int syevd_values(long n, long b, long nb, const double* A, long lda, double* w, 
   if ((size_t)lwork_bytes < P.bytes) return EVD_ERR_WORKSPACE;
   double* base = reinterpret_cast<double*>(work);
   EVD_TRY(pad_prepare(n, A, lda, P, base, st));
+  const int* err = nullptr;
   EVD_TRY(values_core(P.np, b, nb, base + P.oAp, P.np, base + P.owp, work, (long)P.core_bytes,
-                      timed, st));
+                      timed, st, &err));
   EVD_CUDA_TRY(cudaMemcpyAsync(w, base + P.owp, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  EVD_CUDA_TRY(cudaStreamSynchronize(st));
-  return EVD_SUCCESS;
+  return read_device_error(err, st);
 }
 
 }  // namespace evd

@@ -6,9 +6,10 @@ of 1024); this layer adds:
 
 * **any n >= 1** through ``evd_syevd`` itself, which pads an order that is
   not a multiple of nb (or below 64) with a diagonal block above the
-  spectrum, on the device; nb = 32 * 2^k is chosen here as the largest one
-  dividing n' = 32 * ceil(n / 32) (n' >= 64), at most 1024, so the padded
-  order is n'.
+  spectrum, on the device.  nb comes from the measured table of
+  :mod:`evd4sc2025_b200.autotune` (:func:`solve_shape`); without a table it
+  is the largest 32 * 2^k dividing n' = 32 * ceil(n / 32) (n' >= 64), at
+  most 1024 (:func:`padded_shape`).
 * **overlap on the device**: a pool of workers, each with its own CUDA
   stream, one grow-only workspace and padded buffer pair, and a host thread
   (the solver synchronises its own stream a few times per solve; ctypes
@@ -35,7 +36,7 @@ from typing import Callable
 
 import torch
 
-from . import F64, _cm, _ptr, _stream, call, empty_cm, lib
+from . import F64, _cm, _ptr, _stream, autotune, call, empty_cm, lib
 
 MAX_NB = 1024
 
@@ -54,18 +55,29 @@ def padded_shape(n: int) -> tuple[int, int]:
     return np_, nb
 
 
+def solve_shape(n: int) -> tuple[int, int]:
+    """(n', nb) the solver uses for order n: nb from the tuned table when one
+    is present, else the rule of :func:`padded_shape`; n' the padded order."""
+    rule = padded_shape(n)
+    nb = autotune.choose_nb(n, default_nb=rule[1])
+    if nb is None:
+        return rule
+    return autotune.padded_order(n, nb), nb
+
+
 def footprint_bytes(n: int) -> int:
     """Device bytes one solve of order n holds: workspace (with the padded
     copies when n' > n) + A and X of order n + w."""
-    _, nb = padded_shape(n)
+    _, nb = solve_shape(n)
     return int(lib().evd_syevd_work_size(n, 32, nb)) + 2 * n * n * 8 + n * 8
 
 
 class StreamSolver:
-    """One worker: a CUDA stream, one grow-only workspace and one pair of
-    A/X buffers (a smaller problem uses the leading block of the buffers,
-    with their leading dimension), so a worker holds at most the footprint
-    of the largest problem it has solved."""
+    """One worker: a CUDA stream, one grow-only workspace and one A buffer (a
+    smaller problem uses the leading block of the buffer, with its leading
+    dimension), so a worker holds at most the footprint of the largest
+    problem it has solved.  The solver writes w and X straight into freshly
+    allocated result tensors (no copy afterwards)."""
 
     def __init__(self, device="cuda"):
         self.device = torch.device(device)
@@ -73,7 +85,7 @@ class StreamSolver:
         self._ws = None
         self._wsbytes = 0
         self._ld = 0
-        self._A = self._X = self._w = None
+        self._A = None
 
     def _ensure(self, n: int, nb: int):
         need = int(lib().evd_syevd_work_size(n, 32, nb))
@@ -84,35 +96,35 @@ class StreamSolver:
             self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
             self._wsbytes = need
         if n > self._ld:
-            self._A = self._X = self._w = None
+            self._A = None
             self._A = empty_cm(n, n, device=self.device)
-            self._X = empty_cm(n, n, device=self.device)
-            self._w = torch.empty(n, dtype=F64, device=self.device)
             self._ld = n
-        return self._A[:n, :n], self._X[:n, :n], self._w[:n]
+        return self._A[:n, :n]
 
     def release(self):
-        """Drop the workspace and buffers (their memory returns to torch)."""
-        self._ws = self._A = self._X = self._w = None
+        """Drop the workspace and buffer (their memory returns to torch)."""
+        self._ws = self._A = None
         self._wsbytes = self._ld = 0
 
-    def solve(self, A: torch.Tensor):
+    def solve(self, A: torch.Tensor, nb: int | None = None):
         """Eigenvalues (ascending, length n) and eigenvectors (n x n,
         column-major) of the symmetric FP64 matrix A on this worker's stream.
         A may live on the host or the device; results are on the device.
-        Nothing here synchronises the host: the padding runs on the device."""
+        The padding runs on the device; the solver's own host reads are its
+        only synchronisation.  ``nb`` overrides the block size of
+        :func:`solve_shape`."""
         n = A.shape[0]
-        _, nb = padded_shape(n)
+        if nb is None:
+            _, nb = solve_shape(n)
         with torch.cuda.stream(self.stream):
-            Ab, Xb, wb = self._ensure(n, nb)
+            Ab = self._ensure(n, nb)
             Ab.copy_(A, non_blocking=True)
-            pa, lda = _cm(Ab, "A")
-            px, ldx = _cm(Xb, "X")
-            call("evd_syevd", n, 32, nb, pa, lda, _ptr(wb), px, ldx, _ptr(self._ws),
-                 self._wsbytes, 0, _stream(self.stream))
-            w = wb.clone()
+            w = torch.empty(n, dtype=F64, device=self.device)
             X = empty_cm(n, n, device=self.device)
-            X.copy_(Xb)
+            pa, lda = _cm(Ab, "A")
+            px, ldx = _cm(X, "X")
+            call("evd_syevd", n, 32, nb, pa, lda, _ptr(w), px, ldx, _ptr(self._ws),
+                 self._wsbytes, 0, _stream(self.stream))
         return w, X
 
 
@@ -125,7 +137,7 @@ def syevd_any(A: torch.Tensor, solver: StreamSolver | None = None):
 
 
 def syevd_batched(mats: list[torch.Tensor], nstreams: int = 8, device="cuda",
-                  solvers: list[StreamSolver] | None = None):
+                  solvers: list[StreamSolver] | None = None, nb: int | None = None):
     """Eigenpairs of many symmetric matrices of uneven sizes, solved
     concurrently on ``nstreams`` streams.  Returns a list of (w, X) in input
     order (on the device) and the device time of the whole batch in ms
@@ -149,7 +161,7 @@ def syevd_batched(mats: list[torch.Tensor], nstreams: int = 8, device="cuda",
                     i = next(nxt, None)
                 if i is None:
                     break
-                out[i] = sv.solve(mats[i])
+                out[i] = sv.solve(mats[i], nb)
         except BaseException as e:  # surfaced to the caller below
             errors.append(e)
         ev = torch.cuda.Event(enable_timing=True)

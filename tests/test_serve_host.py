@@ -82,3 +82,45 @@ def test_poisson_stream_is_seeded():
     assert all(64 <= r.A.shape[0] <= 256 for r in a)
     assert all(x.arrival < y.arrival for x, y in zip(a, a[1:]))
     assert torch.equal(a[3].A, b[3].A) and torch.equal(a[3].A, a[3].A.t())
+
+
+def test_autotune_choice_rules():
+    """choose_nb scales each candidate's time by the cube of the padded order
+    it needs, so a size just above a multiple of a large nb takes a smaller
+    one; without a table the rule applies."""
+    from evd4sc2025_b200 import autotune
+    table = {"b": 32, "entries": [
+        {"n": 1024, "nb": 1024, "ms": {"32": 30.0, "256": 12.0, "1024": 10.0}},
+        {"n": 4096, "nb": 256, "ms": {"32": 200.0, "256": 80.0, "1024": 90.0}}]}
+    assert autotune.choose_nb(1000, table) == 1024
+    assert autotune.choose_nb(1030, table) == 256   # nb 1024 would pad to 2048
+    assert autotune.choose_nb(4096, table) == 256
+    assert autotune.choose_nb(1, table) in (32, 256, 1024)
+    assert autotune.choose_nb(500, {"entries": []}) is None
+    # the rule's choice stands unless the table beats it by more than 5 %
+    assert autotune.choose_nb(1024, table, default_nb=256) == 1024  # 10 vs 12: tuned wins
+    assert autotune.choose_nb(4096, table, default_nb=1024) == 256  # 80 vs 90: tuned wins
+    assert autotune.choose_nb(4096, table, default_nb=64) == 64     # no time for 64: rule
+    near = {"entries": [{"n": 512, "nb": 256, "ms": {"256": 10.0, "512": 10.3}}]}
+    assert autotune.choose_nb(512, near, default_nb=512) == 512     # within 5 %: rule
+    assert autotune.padded_order(1, 32) == 64 and autotune.padded_order(1030, 256) == 1280
+    sizes = autotune.default_sizes(64, 8192, 3)
+    assert sizes[0] == 64 and sizes[-1] == 8192 and len(sizes) == 22
+
+
+def test_solve_shape_is_a_valid_padding():
+    for n in (1, 63, 64, 65, 1000, 1056, 3000, 8192):
+        np_, nb = serve.solve_shape(n)
+        assert np_ >= n and np_ % nb == 0 and (nb // 32) & (nb // 32 - 1) == 0
+
+
+def test_autotune_active_table_switch():
+    from evd4sc2025_b200 import autotune
+    t = {"entries": [{"n": 512, "nb": 64, "ms": {"64": 1.0, "512": 2.0}}]}
+    try:
+        autotune.use_table(t)
+        assert autotune.choose_nb(512) == 64 and serve.solve_shape(512) == (512, 64)
+        autotune.use_table(None)
+        assert autotune.choose_nb(512) is None and serve.solve_shape(512) == serve.padded_shape(512)
+    finally:
+        autotune._cached = autotune._cached_path = None
