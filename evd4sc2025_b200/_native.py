@@ -55,6 +55,14 @@ SIGNATURES = {
     "evd_stebz": (_i, [_l, _p, _p, _p, _p, _l, _p]),
     "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
+    "evd_panel_qr_lp_work_size": (_l, [_l, _l]),
+    "evd_panel_qr_s": (_i, [_l, _l, _p, _l, _p, _l, _p, _l, _p, _l, _p]),
+    "evd_panel_qr_h": (_i, [_l, _l, _p, _l, _p, _l, _p, _l, _p, _l, _p]),
+    "evd_tsqr_s": (_i, [_l, _l, _p, _l, _p, _l, _p, _l, _p]),
+    "evd_tsqr_h": (_i, [_l, _l, _p, _l, _p, _l, _p, _l, _p]),
+    "evd_syr2k_lower_s": (_i, [_l, _l, C.c_float, _p, _l, _p, _l, C.c_float, _p, _l, _l, _p]),
+    "evd_tc_syr2k": (_i, [_l, _l, C.c_float, _p, _l, _p, _l, C.c_float, _p, _l, _p, _l, _p]),
+    "evd_syr2k_lower_h": (_i, [_l, _l, C.c_float, _p, _l, _p, _l, C.c_float, _p, _l, _l, _p]),
     "evd_write_matrix_bin": (_i, [C.c_char_p, _i, _l, _l, _p, _l]),
     "evd_matrix_bin_count": (_l, [C.c_char_p]),
     "evd_matrix_bin_shape": (_i, [C.c_char_p, _l, C.POINTER(_l), C.POINTER(_l)]),

@@ -1,0 +1,557 @@
+// Reduced-precision entry points of the reference's public API.
+//
+// The reference instantiates its panel QR and trailing SYR2K for float and
+// half besides double (api/panelQR.cu:262-701, api/TCblas/tc_ozimmu_syr2k.cu:
+// 343-629 and :683-720) and has a mixed update `tc_syr2k` (FP32 data, FP16
+// tensor-core products, FP32 accumulation; api/TCblas/tc_syr2k.cu:144-330).
+// The B200 versions:
+//
+// * tc_syr2k and the half SYR2K run one tcgen05 kernel: both operands are
+//   rounded to FP16 while they are staged into shared memory (so the FP16
+//   copy the reference makes in `hwork` first is not needed), each 64-wide K
+//   chunk is multiplied by `tcgen05.mma.kind::f16` into a 128 x 128 FP32
+//   accumulator in tensor memory, and the epilogue applies alpha / beta on
+//   the lower triangle.  A B^T + B A^T is one product over the concatenated
+//   K range: [A | B] * [B | A]^T.
+// * the FP32 SYR2K is a SIMT FP32 kernel (exact FP32 multiply-add, the
+//   arithmetic of CUBLAS_COMPUTE_32F that the reference asks cuBLAS for).
+// * the FP32 / FP16 panel QR and TSQR convert the panel to FP64, run the
+//   FP64 panel kernels (the panel is latency-bound: FP64 costs nothing there
+//   and is more accurate) and round the results back.
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "panel_qr.cuh"
+
+namespace evd {
+namespace {
+
+// ------------------------------------------------------------ conversions
+__device__ __forceinline__ double to_d(float x) { return (double)x; }
+__device__ __forceinline__ double to_d(__half x) { return (double)__half2float(x); }
+__device__ __forceinline__ void from_d(double x, float* p) { *p = (float)x; }
+__device__ __forceinline__ void from_d(double x, __half* p) { *p = __double2half(x); }
+
+template <typename T>
+__global__ void to_double_kernel(long m, long n, const T* __restrict__ src, long lds,
+                                 double* __restrict__ dst, long ldd) {
+  for (long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x)
+      dst[i + j * ldd] = to_d(src[i + j * lds]);
+}
+
+template <typename T>
+__global__ void from_double_kernel(long m, long n, const double* __restrict__ src, long lds,
+                                   T* __restrict__ dst, long ldd) {
+  for (long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m; i += (long)gridDim.x * blockDim.x)
+      from_d(src[i + j * lds], dst + i + j * ldd);
+}
+
+template <typename T>
+int to_double(long m, long n, const T* src, long lds, double* dst, long ldd, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return EVD_SUCCESS;
+  dim3 g((unsigned)std::min<long>(ceil_div_i(m, 256), 1024), (unsigned)std::min<long>(n, 65535));
+  to_double_kernel<T><<<g, 256, 0, st>>>(m, n, src, lds, dst, ldd);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+template <typename T>
+int from_double(long m, long n, const double* src, long lds, T* dst, long ldd, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return EVD_SUCCESS;
+  dim3 g((unsigned)std::min<long>(ceil_div_i(m, 256), 1024), (unsigned)std::min<long>(n, 65535));
+  from_double_kernel<T><<<g, 256, 0, st>>>(m, n, src, lds, dst, ldd);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+// --------------------------------------------------- panel QR in FP32/FP16
+// Workspace in doubles: A, W (m x 32), R (32 x 32), then the FP64 panel's.
+long lp_panel_ws_doubles(long m) { return 2 * m * 32 + 32 * 32 + 32 + panel_qr_ws_doubles(m); }
+
+template <typename T>
+int lp_panel(long m, long n, T* A, long lda, T* W, long ldw, T* R, long ldr, void* work,
+             long lwork_bytes, bool form_wy, cudaStream_t st) {
+  EVD_TRY(panel_qr_check(m, n, lda));
+  if (!A || !R || !work || ldr < n || (form_wy && (!W || ldw < m))) return EVD_ERR_INVALID_ARG;
+  if (lwork_bytes < (long)sizeof(double) * lp_panel_ws_doubles(m)) return EVD_ERR_WORKSPACE;
+  double* base = reinterpret_cast<double*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  // the alignment step may cost up to 255 bytes: the size query adds 32 doubles
+  double* Ad = base;
+  double* Wd = Ad + m * 32;
+  double* Rd = Wd + m * 32;
+  double* ws = Rd + 32 * 32;
+  EVD_TRY(to_double(m, 32, A, lda, Ad, m, st));
+  EVD_TRY(panel_counters_reset(m, ws, st));
+  if (form_wy) {
+    EVD_TRY(panel_qr_launch(m, Ad, m, ws, 1, Ad, m, Wd, m, Rd, 32, nullptr, 0, st));
+    EVD_TRY(from_double(m, 32, Wd, m, W, ldw, st));
+  } else {
+    EVD_TRY(panel_qr_launch(m, Ad, m, ws, 0, nullptr, 0, nullptr, 0, Rd, 32, nullptr, 0, st));
+  }
+  EVD_TRY(from_double(m, 32, Ad, m, A, lda, st));
+  EVD_TRY(from_double(32, 32, Rd, 32, R, ldr, st));
+  return EVD_SUCCESS;
+}
+
+// ------------------------------------------------------- FP32 SIMT SYR2K
+// C(lower) = alpha * [A | B] [B | A]^T + beta * C over lower-triangle tiles
+// of 128 x 128; 256 threads, 8 x 8 outputs per thread, K chunks of 8 staged
+// in shared memory (double-buffered).
+constexpr int kSB = 128;  // tile edge
+constexpr int kSK = 8;    // K chunk
+
+__device__ __forceinline__ void tri_tile(long p, long& bi, long& bj) {
+  // p -> (bi >= bj) with p = bi (bi + 1) / 2 + bj
+  long i = (long)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+  while (i * (i + 1) / 2 > p) --i;
+  while ((i + 1) * (i + 2) / 2 <= p) ++i;
+  bi = i;
+  bj = p - i * (i + 1) / 2;
+}
+
+// element kk (0 <= kk < 2k) of row r of the left ([A|B]) or right ([B|A]) operand
+template <typename T>
+__device__ __forceinline__ float cat_elem(const T* __restrict__ P, long ldp, const T* __restrict__ Q,
+                                          long ldq, long n, long k, long r, long kk) {
+  if (r >= n) return 0.0f;
+  if (kk < k) return (float)P[r + kk * ldp];
+  kk -= k;
+  if (kk < k) return (float)Q[r + kk * ldq];
+  return 0.0f;
+}
+
+__global__ void __launch_bounds__(256) ssyr2k_kernel(long n, long k, float alpha,
+                                                     const float* __restrict__ A, long lda,
+                                                     const float* __restrict__ B, long ldb,
+                                                     float beta, float* __restrict__ C, long ldc) {
+  __shared__ __align__(16) float Ls[2][kSK][kSB];
+  __shared__ __align__(16) float Rs[2][kSK][kSB];
+  long bi, bj;
+  tri_tile(blockIdx.x, bi, bj);
+  const long m0 = bi * kSB, n0 = bj * kSB;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads, 8 x 8 each
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+  const long K2 = 2 * k;
+  const long nk = (K2 + kSK - 1) / kSK;
+  // staging: each thread loads 4 elements of each operand per chunk
+  // (row = tid & 127, kk = (tid >> 7) * 4 + q)
+  const int lr = tid & 127, lk = (tid >> 7) * 4;
+  auto load = [&](long c, float* lv, float* rv) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const long kk = c * kSK + lk + q;
+      lv[q] = cat_elem(A, lda, B, ldb, n, k, m0 + lr, kk);
+      rv[q] = cat_elem(B, ldb, A, lda, n, k, n0 + lr, kk);
+    }
+  };
+  float lv[4], rv[4];
+  load(0, lv, rv);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    Ls[0][lk + q][lr] = lv[q];
+    Rs[0][lk + q][lr] = rv[q];
+  }
+  __syncthreads();
+  for (long c = 0; c < nk; ++c) {
+    const int buf = (int)(c & 1);
+    if (c + 1 < nk) load(c + 1, lv, rv);
+#pragma unroll
+    for (int kk = 0; kk < kSK; ++kk) {
+      float a[8], b[8];
+      *reinterpret_cast<float4*>(a) = *reinterpret_cast<const float4*>(&Ls[buf][kk][ty * 4]);
+      *reinterpret_cast<float4*>(a + 4) = *reinterpret_cast<const float4*>(&Ls[buf][kk][64 + ty * 4]);
+      *reinterpret_cast<float4*>(b) = *reinterpret_cast<const float4*>(&Rs[buf][kk][tx * 4]);
+      *reinterpret_cast<float4*>(b + 4) = *reinterpret_cast<const float4*>(&Rs[buf][kk][64 + tx * 4]);
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    if (c + 1 < nk) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        Ls[buf ^ 1][lk + q][lr] = lv[q];
+        Rs[buf ^ 1][lk + q][lr] = rv[q];
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const long gi = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const long gj = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
+      if (gi < n && gj <= gi) {
+        float* c = C + gi + gj * ldc;
+        *c = (beta == 0.0f) ? alpha * acc[i][j] : fmaf(alpha, acc[i][j], beta * *c);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------ tcgen05 FP16 SYR2K (TMEM)
+// Tile 128 x 128 of C per CTA (128 threads), K chunks of 64 staged as FP16 in
+// the canonical K-major layout without swizzle: core matrices of 8 rows x 16
+// bytes (128 contiguous bytes), core (row group g, K core c) at
+// (g * 8 + c) * 128 bytes, so the leading (K) byte offset is 128 and the
+// stride (row-group) byte offset is 1024.  One elected thread issues four
+// M128 N128 K16 MMAs per chunk and commits them to the chunk's mbarrier;
+// three stages let the staging of chunk t+1, t+2 overlap the MMAs of chunk t.
+constexpr int kTM = 128, kTN = 128, kTK = 64, kTStages = 3, kTThreads = 128;
+constexpr int kTTileBytes = kTM * kTK * 2;          // 16 KB per operand tile
+constexpr int kTStageBytes = 2 * kTTileBytes;        // left + right
+constexpr int kTSmem = kTStages * kTStageBytes + 256;  // + barriers, TMEM slot, alignment
+constexpr unsigned long long kTWaitNs = 2000000000ull;  // 2 s per wait: far above any chunk
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase `parity`; false after kTWaitNs (error recorded).
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63u) == 63u && gtimer() - t0 > kTWaitNs) {
+      atomicExch(err, kDevTimeoutTree);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  // start >> 4 | LBO (128 B) >> 4 << 16 | SBO (1024 B) >> 4 << 32 | version 1 << 46;
+  // base offset 0, no swizzle
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B F16 (0),
+// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kTN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
+__device__ __forceinline__ float ld_elem(const __half* p) { return __half2float(p[0]); }
+
+// Stage rows [r0, r0 + 128) x K-chunk [kk0, kk0 + 64) of P (n x k) as FP16
+// into `tile` (K-major canonical layout), zero beyond row n and column k.
+// Thread t owns row t: 8 K cores of 8 values, each one 16-byte core row.
+template <typename T>
+__device__ __forceinline__ void stage_rows(uint8_t* tile, const T* __restrict__ P, long ldp, long n,
+                                           long k, long r0, long kk0) {
+  const int t = threadIdx.x;
+  const long r = r0 + t;
+  const bool rok = r < n;
+  uint8_t* rowbase = tile + (t >> 3) * 1024 + (t & 7) * 16;
+#pragma unroll 2
+  for (int c = 0; c < 8; ++c) {
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long kk = kk0 + c * 8 + q;
+      v[q] = (rok && kk < k) ? ld_elem(P + r + kk * ldp) : 0.0f;
+    }
+    __half2 h[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) h[q] = __floats2half2_rn(v[2 * q], v[2 * q + 1]);
+    *reinterpret_cast<uint4*>(rowbase + c * 128) = *reinterpret_cast<const uint4*>(h);
+  }
+}
+
+__device__ __forceinline__ void store_c(float* c, float v, float alpha, float beta) {
+  *c = (beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * *c);
+}
+__device__ __forceinline__ void store_c(__half* c, float v, float alpha, float beta) {
+  *c = __float2half_rn((beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * __half2float(*c)));
+}
+
+template <typename TI, typename TC>
+__global__ void __launch_bounds__(kTThreads) tc_syr2k_kernel(long n, long k, float alpha,
+                                                             const TI* __restrict__ A, long lda,
+                                                             const TI* __restrict__ B, long ldb,
+                                                             float beta, TC* __restrict__ C,
+                                                             long ldc, int* err) {
+  extern __shared__ __align__(1024) uint8_t tsm[];
+  uint8_t* stages = tsm;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tsm + kTStages * kTStageBytes);  // kTStages + 1
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kTStages + 1);
+  long bi, bj;
+  tri_tile(blockIdx.x, bi, bj);
+  const long m0 = bi * kTM, n0 = bj * kTN;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (tid == 0) {
+    for (int s = 0; s <= kTStages; ++s) mbar_init(bars + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)),
+                 "r"(kTN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const long kc = (k + kTK - 1) / kTK;  // chunks per half of [A | B]
+  const long nch = 2 * kc;
+  bool ok = true;
+  for (long t = 0; t < nch && ok; ++t) {
+    const int s = (int)(t % kTStages);
+    uint8_t* Lt = stages + s * kTStageBytes;
+    uint8_t* Rt = Lt + kTTileBytes;
+    if (t >= kTStages) ok = mbar_wait(bars + s, (uint32_t)((t / kTStages - 1) & 1), err);
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
+    // chunk t of the concatenated K range: the first kc chunks come from
+    // (A, B), the last kc from (B, A); each half is zero-padded to kc * 64
+    const long kk0 = (t < kc) ? t * kTK : (t - kc) * kTK;
+    if (t < kc) {
+      stage_rows(Lt, A, lda, n, k, m0, kk0);
+      stage_rows(Rt, B, ldb, n, k, n0, kk0);
+    } else {
+      stage_rows(Lt, B, ldb, n, k, m0, kk0);
+      stage_rows(Rt, A, lda, n, k, n0, kk0);
+    }
+    // make the generic-proxy shared stores visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t la = smem_u32(Lt), ra = smem_u32(Rt);
+#pragma unroll
+      for (int ks = 0; ks < kTK / 16; ++ks)
+        umma_f16(tmem, smem_desc(la + ks * 256), smem_desc(ra + ks * 256),
+                 (t > 0 || ks > 0) ? 1u : 0u);
+      umma_commit(bars + s);
+    }
+  }
+  // all MMAs issued by thread 0 complete -> the done barrier
+  if (tid == 0) umma_commit(bars + kTStages);
+  const bool done = mbar_wait(bars + kTStages, 0, err);
+  ok = __syncthreads_and(ok && done);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    // epilogue: warp w reads TMEM lanes 32w .. 32w + 31 (rows of the tile)
+    const long gi = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTN; c0 += 16) {
+      uint32_t v[16];
+      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+          "%11, %12, %13, %14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (gi < n) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const long gj = n0 + c0 + j;
+          if (gj <= gi) store_c(C + gi + gj * ldc, __uint_as_float(v[j]), alpha, beta);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTN)
+                 : "memory");
+}
+
+template <typename TI, typename TC>
+int tc_syr2k_launch(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
+                    float beta, TC* C, long ldc, int* err, cudaStream_t st) {
+  const long T = (n + kTM - 1) / kTM;
+  const long tiles = T * (T + 1) / 2;
+  EVD_CUDA_TRY(cudaFuncSetAttribute(tc_syr2k_kernel<TI, TC>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kTSmem));
+  tc_syr2k_kernel<TI, TC><<<(unsigned)tiles, kTThreads, kTSmem, st>>>(n, k, alpha, A, lda, B, ldb,
+                                                                     beta, C, ldc, err);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+bool syr2k_args_ok(long n, long k, const void* A, long lda, const void* B, long ldb,
+                   const void* C, long ldc) {
+  if (n < 0 || k < 0 || ldc < std::max(1L, n)) return false;
+  if (n > 0 && !C) return false;
+  if (n > 0 && k > 0 && (!A || !B || lda < n || ldb < n)) return false;
+  return (n + kTM - 1) / kTM < (1L << 15);  // tile pairs fit one grid dimension
+}
+
+// Scale C(lower) by beta (k == 0: no product).
+template <typename TC>
+__global__ void scale_lower_kernel(long n, float beta, TC* C, long ldc) {
+  for (long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long i = j + blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+      store_c(C + i + j * ldc, 0.0f, 0.0f, beta);
+}
+
+template <typename TC>
+int scale_lower(long n, float beta, TC* C, long ldc, cudaStream_t st) {
+  if (n <= 0) return EVD_SUCCESS;
+  dim3 g((unsigned)std::min<long>(ceil_div_i(n, 256), 1024), (unsigned)std::min<long>(n, 65535));
+  scale_lower_kernel<TC><<<g, 256, 0, st>>>(n, beta, C, ldc);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+// error word for the bounded waits of the tensor-core kernel (one per device
+// is enough: it only changes when a wait gives up)
+int* tc_err_word() {
+  static int* dev_word[64] = {nullptr};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+  if (!dev_word[d]) {
+    int* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+    if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) return nullptr;
+    dev_word[d] = p;
+  }
+  return dev_word[d];
+}
+
+int check_tc_err(int* err, cudaStream_t st) {
+  int h = 0;
+  EVD_CUDA_TRY(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EVD_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h != 0) {
+    cudaMemsetAsync(err, 0, sizeof(int), st);
+    return EVD_ERR_TIMEOUT;
+  }
+  return EVD_SUCCESS;
+}
+
+}  // namespace
+}  // namespace evd
+
+using evd::lp_panel;
+
+// ---------------------------------------------------------------- C ABI
+extern "C" long evd_panel_qr_lp_work_size(long m, long n) {
+  if (evd::panel_qr_check(m, n, m) != EVD_SUCCESS) return 0;
+  return (long)sizeof(double) * evd::lp_panel_ws_doubles(m);
+}
+
+extern "C" int evd_panel_qr_s(long m, long n, float* A, long lda, float* W, long ldw, float* R,
+                              long ldr, void* work, long lwork_bytes, cudaStream_t stream) {
+  return lp_panel(m, n, A, lda, W, ldw, R, ldr, work, lwork_bytes, true, stream);
+}
+
+extern "C" int evd_panel_qr_h(long m, long n, void* A, long lda, void* W, long ldw, void* R,
+                              long ldr, void* work, long lwork_bytes, cudaStream_t stream) {
+  return lp_panel(m, n, (__half*)A, lda, (__half*)W, ldw, (__half*)R, ldr, work, lwork_bytes,
+                  true, stream);
+}
+
+extern "C" int evd_tsqr_s(long m, long n, float* A, long lda, float* R, long ldr, void* work,
+                          long lwork_bytes, cudaStream_t stream) {
+  return lp_panel(m, n, A, lda, (float*)nullptr, 0, R, ldr, work, lwork_bytes, false, stream);
+}
+
+extern "C" int evd_tsqr_h(long m, long n, void* A, long lda, void* R, long ldr, void* work,
+                          long lwork_bytes, cudaStream_t stream) {
+  return lp_panel(m, n, (__half*)A, lda, (__half*)nullptr, 0, (__half*)R, ldr, work, lwork_bytes,
+                  false, stream);
+}
+
+extern "C" int evd_syr2k_lower_s(long n, long k, float alpha, const float* A, long lda,
+                                 const float* B, long ldb, float beta, float* C, long ldc, long nb,
+                                 cudaStream_t stream) {
+  (void)nb;
+  if (!evd::syr2k_args_ok(n, k, A, lda, B, ldb, C, ldc)) return EVD_ERR_INVALID_ARG;
+  if (n == 0) return EVD_SUCCESS;
+  if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, C, ldc, stream);
+  const long T = (n + evd::kSB - 1) / evd::kSB;
+  evd::ssyr2k_kernel<<<(unsigned)(T * (T + 1) / 2), 256, 0, stream>>>(n, k, alpha, A, lda, B, ldb,
+                                                                     beta, C, ldc);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+extern "C" int evd_tc_syr2k(long n, long k, float alpha, const float* A, long lda, const float* B,
+                            long ldb, float beta, float* C, long ldc, void* hwork, long nb,
+                            cudaStream_t stream) {
+  (void)hwork;
+  (void)nb;
+  if (!evd::syr2k_args_ok(n, k, A, lda, B, ldb, C, ldc)) return EVD_ERR_INVALID_ARG;
+  if (n == 0) return EVD_SUCCESS;
+  if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, C, ldc, stream);
+  int* err = evd::tc_err_word();
+  if (!err) return EVD_ERR_CUDA;
+  EVD_TRY(evd::tc_syr2k_launch(n, k, alpha, A, lda, B, ldb, beta, C, ldc, err, stream));
+  return evd::check_tc_err(err, stream);
+}
+
+extern "C" int evd_syr2k_lower_h(long n, long k, float alpha, const void* A, long lda,
+                                 const void* B, long ldb, float beta, void* C, long ldc, long nb,
+                                 cudaStream_t stream) {
+  (void)nb;
+  if (!evd::syr2k_args_ok(n, k, A, lda, B, ldb, C, ldc)) return EVD_ERR_INVALID_ARG;
+  if (n == 0) return EVD_SUCCESS;
+  if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, (__half*)C, ldc, stream);
+  int* err = evd::tc_err_word();
+  if (!err) return EVD_ERR_CUDA;
+  EVD_TRY(evd::tc_syr2k_launch(n, k, alpha, (const __half*)A, lda, (const __half*)B, ldb, beta,
+                               (__half*)C, ldc, err, stream));
+  return evd::check_tc_err(err, stream);
+}

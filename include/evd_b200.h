@@ -263,6 +263,42 @@ int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, dou
 int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
                      long lwork_bytes, int timed, cudaStream_t stream);
 
+/* ---- FP32 / FP16 entry points of the reference's API -------------------- */
+
+/* The reference instantiates panelQR and tc_ozimmu_syr2k for float and half
+ * (api/panelQR.cu:262-701, api/TCblas/tc_ozimmu_syr2k.cu:343-629, :683-720)
+ * and has tc_syr2k (api/inc/tc_syr2k.h:6-18, api/TCblas/tc_syr2k.cu:144-330).
+ * FP16 matrices are passed as void* holding IEEE binary16 values. */
+
+/* Bytes of workspace for evd_panel_qr_s/_h and evd_tsqr_s/_h (m x 32 panel). */
+long evd_panel_qr_lp_work_size(long m, long n);
+/* panelQR<float> / panelQR<half> (api/inc/PanelQR.h:7-18), n == 32: A <- Y,
+ * W, R as evd_panel_qr.  Computed in FP64 on converted copies, rounded back. */
+int evd_panel_qr_s(long m, long n, float* A, long lda, float* W, long ldw, float* R, long ldr,
+                   void* work, long lwork_bytes, cudaStream_t stream);
+int evd_panel_qr_h(long m, long n, void* A, long lda, void* W, long ldw, void* R, long ldr,
+                   void* work, long lwork_bytes, cudaStream_t stream);
+/* hou_tsqr_panel<float/half, 128, 32>: A <- explicit thin Q, R. */
+int evd_tsqr_s(long m, long n, float* A, long lda, float* R, long ldr, void* work,
+               long lwork_bytes, cudaStream_t stream);
+int evd_tsqr_h(long m, long n, void* A, long lda, void* R, long ldr, void* work,
+               long lwork_bytes, cudaStream_t stream);
+/* tc_ozimmu_syr2k<float>: C(lower) = alpha (A B^T + B A^T) + beta C in FP32
+ * arithmetic (SIMT FP32 FMA; CUBLAS_COMPUTE_32F in the reference).  Only the
+ * lower triangle (with the diagonal) is written; beta == 0 does not read C. */
+int evd_syr2k_lower_s(long n, long k, float alpha, const float* A, long lda, const float* B,
+                      long ldb, float beta, float* C, long ldc, long nb, cudaStream_t stream);
+/* tc_syr2k: as above with A and B rounded to FP16 and the products summed in
+ * FP32 on the tcgen05 tensor cores.  The rounding happens while the operands
+ * are staged on chip, so `hwork` (the reference's FP16 copy, 2 n k halves) is
+ * accepted and not used; nb is accepted and not needed. */
+int evd_tc_syr2k(long n, long k, float alpha, const float* A, long lda, const float* B, long ldb,
+                 float beta, float* C, long ldc, void* hwork, long nb, cudaStream_t stream);
+/* tc_ozimmu_syr2k<half>: FP16 A, B, C; FP32 accumulation on the tensor cores
+ * (the reference accumulates in FP16, CUBLAS_COMPUTE_16F); alpha, beta as float. */
+int evd_syr2k_lower_h(long n, long k, float alpha, const void* A, long lda, const void* B,
+                      long ldb, float beta, void* C, long ldc, long nb, cudaStream_t stream);
+
 /* ---- Matrix and eigenpair files ----------------------------------------- */
 
 /* The reference has CSV only (writeMatrixToCsvV2, util/inc/fileOpTool.h:51-80;

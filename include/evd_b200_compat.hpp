@@ -6,6 +6,8 @@
 // the reference's way (message + exit), see EVD_COMPAT_CHECK.
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <cstdio>
 #include <cstdlib>
 
@@ -64,11 +66,37 @@ inline void panelQR<double>(cusolverDnHandle_t, cublasHandle_t, long m, long n, 
                                 evd_panel_qr_work_size(m, n), nullptr));
 }
 
+// panelQR<float> / panelQR<half> (api/panelQR.cu:262-701), n == 32.  `work`
+// must hold evd_panel_qr_lp_work_size(m, n) bytes.
+template <>
+inline void panelQR<float>(cusolverDnHandle_t, cublasHandle_t, long m, long n, float* A,
+                           long lda, float* W, long ldw, float* R, long ldr, float* work,
+                           int* /*info*/) {
+  EVD_COMPAT_CHECK(evd_panel_qr_s(m, n, A, lda, W, ldw, R, ldr, work,
+                                  evd_panel_qr_lp_work_size(m, n), nullptr));
+}
+
+template <>
+inline void panelQR<__half>(cusolverDnHandle_t, cublasHandle_t, long m, long n, __half* A,
+                            long lda, __half* W, long ldw, __half* R, long ldr, __half* work,
+                            int* /*info*/) {
+  EVD_COMPAT_CHECK(evd_panel_qr_h(m, n, A, lda, W, ldw, R, ldr, work,
+                                  evd_panel_qr_lp_work_size(m, n), nullptr));
+}
+
 // api/inc/TallShinnyQR.h:9-17 (M = 128, N = 32 is the only instantiation used).
 template <typename T, long M, long N>
 void hou_tsqr_panel(cublasHandle_t, long m, long n, T* A, long lda, T* R, long ldr, T* work) {
   static_assert(M == 128 && N == 32, "evd_b200 implements the 128 x 32 TSQR");
-  EVD_COMPAT_CHECK(evd_tsqr(m, n, A, lda, R, ldr, work, evd_panel_qr_work_size(m, n), nullptr));
+  if constexpr (sizeof(T) == 8) {
+    EVD_COMPAT_CHECK(evd_tsqr(m, n, A, lda, R, ldr, work, evd_panel_qr_work_size(m, n), nullptr));
+  } else if constexpr (sizeof(T) == 4) {
+    EVD_COMPAT_CHECK(evd_tsqr_s(m, n, A, lda, R, ldr, work, evd_panel_qr_lp_work_size(m, n),
+                                nullptr));
+  } else {
+    EVD_COMPAT_CHECK(evd_tsqr_h(m, n, A, lda, R, ldr, work, evd_panel_qr_lp_work_size(m, n),
+                                nullptr));
+  }
 }
 
 // api/inc/tc_ozimmu_syr2k.h:6-18: C(lower) = alpha (A B^T + B A^T) + beta C,
@@ -82,6 +110,27 @@ inline void tc_ozimmu_syr2k<double>(cublasHandle_t, long n, long k, double alpha
                                     long lda, double* B, long ldb, double beta, double* C,
                                     long ldc, long nb) {
   EVD_COMPAT_CHECK(evd_syr2k_lower_mirror(n, k, alpha, A, lda, B, ldb, beta, C, ldc, nb, nullptr));
+}
+
+template <>
+inline void tc_ozimmu_syr2k<float>(cublasHandle_t, long n, long k, float alpha, float* A,
+                                   long lda, float* B, long ldb, float beta, float* C, long ldc,
+                                   long nb) {
+  EVD_COMPAT_CHECK(evd_syr2k_lower_s(n, k, alpha, A, lda, B, ldb, beta, C, ldc, nb, nullptr));
+}
+
+template <>
+inline void tc_ozimmu_syr2k<__half>(cublasHandle_t, long n, long k, __half alpha, __half* A,
+                                    long lda, __half* B, long ldb, __half beta, __half* C,
+                                    long ldc, long nb) {
+  EVD_COMPAT_CHECK(evd_syr2k_lower_h(n, k, __half2float(alpha), A, lda, B, ldb,
+                                     __half2float(beta), C, ldc, nb, nullptr));
+}
+
+// api/inc/tc_syr2k.h:6-18: FP16 products, FP32 accumulation; hwork unused.
+inline void tc_syr2k(cublasHandle_t, long n, long k, float alpha, float* A, long lda, float* B,
+                     long ldb, float beta, float* C, long ldc, __half* hwork, long nb) {
+  EVD_COMPAT_CHECK(evd_tc_syr2k(n, k, alpha, A, lda, B, ldb, beta, C, ldc, hwork, nb, nullptr));
 }
 
 // api/inc/BC_backTrans.h:3 — same name, same arguments, same return value.
