@@ -45,13 +45,19 @@ def to_cm(t: torch.Tensor, dtype, device="cuda") -> torch.Tensor:
 
 
 def tc_syr2k(alpha: float, A: torch.Tensor, B: torch.Tensor, beta: float, Cm: torch.Tensor,
-             nb: int = 0, stream=None) -> torch.Tensor:
-    """C(lower) = alpha (A B^T + B A^T) + beta C with FP16 products (FP32 data)."""
+             nb: int = 0, stream=None, hwork=True) -> torch.Tensor:
+    """C(lower) = alpha (A B^T + B A^T) + beta C with FP16 products (FP32 data).
+
+    ``hwork``: the reference's FP16 workspace (2 n k halves); True allocates
+    it, None runs without one (operands rounded while staged)."""
     n, k = A.shape
     pa, lda = _cm(A, "A", (torch.float32,))
     pb, ldb = _cm(B, "B", (torch.float32,))
     pc, ldc = _cm(Cm, "C", (torch.float32,))
-    call("evd_tc_syr2k", n, k, alpha, pa, lda, pb, ldb, beta, pc, ldc, None, nb, _stream(stream))
+    if hwork is True:
+        hwork = torch.empty(max(1, 2 * n * k), dtype=torch.float16, device=A.device)
+    ph = None if hwork is None else C.c_void_p(hwork.data_ptr())
+    call("evd_tc_syr2k", n, k, alpha, pa, lda, pb, ldb, beta, pc, ldc, ph, nb, _stream(stream))
     return Cm
 
 

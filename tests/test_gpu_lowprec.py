@@ -49,15 +49,18 @@ def _check_lower(Cout, C0, ref, bound, k, extra_rel=0.0):
 
 
 @pytest.mark.parametrize("n,k", [(1, 1), (100, 7), (128, 64), (300, 200), (1000, 256),
-                                 (513, 1024)])
+                                 (513, 1024), (200, 40), (129, 8)])
 @pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (0.5, 0.0), (2.0, -0.25)])
-def test_tc_syr2k(cuda, evdlib, n, k, alpha, beta):
+@pytest.mark.parametrize("packed", [True, False])
+def test_tc_syr2k(cuda, evdlib, n, k, alpha, beta, packed):
+    """packed: operands packed into the FP16 workspace and streamed by cp.async
+    (k % 8 == 0; other k take the staged path); else rounded while staged."""
     A, B, Cm = _data(n, k, n * 7 + k, cuda)
     if beta == 0.0:
         Cm.fill_(float("nan"))  # beta == 0 must not read C (lower NaN, upper 0)
         Cm.tril_()
     C0 = Cm.clone()
-    LP.tc_syr2k(alpha, A, B, beta, Cm)
+    LP.tc_syr2k(alpha, A, B, beta, Cm, hwork=True if packed else None)
     torch.cuda.synchronize()
     Ah, Bh = A.half().double().cpu(), B.half().double().cpu()
     Cd = torch.nan_to_num(C0.double().cpu()) if beta == 0.0 else C0.double().cpu()
