@@ -33,6 +33,7 @@ __all__ = [
     "EvdError", "lib", "empty_cm", "to_cm", "dgemm", "syr2k", "band_pack", "bulge_chase",
     "tsqr", "panel_qr", "sy2sb", "stedc", "bc_back", "bc_back_apply", "wy_from_slide",
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
+    "syevd_values", "eigvalsh", "stebz", "refine_syev",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -389,6 +390,24 @@ def syevd_values(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | N
 
 
 eigvalsh = syevd_values
+
+
+def refine_syev(A: torch.Tensor, X: torch.Tensor, iters: int = 2, w: torch.Tensor | None = None,
+                stream=None):
+    """Ogita-Aishima refinement of approximate eigenvectors X (in place) of
+    the symmetric FP64 matrix A; returns (w, X) with w the refined
+    eigenvalues in the column order of X."""
+    n = A.shape[0]
+    nw = int(lib().evd_refine_syev_work_size(n))
+    if nw <= 0:
+        raise EvdError("evd_refine_syev_work_size", -1)
+    work = torch.empty(nw, dtype=F64, device=A.device)
+    if w is None:
+        w = torch.empty(n, dtype=F64, device=A.device)
+    pa, lda = _cm(A, "A")
+    px, ldx = _cm(X, "X")
+    call("evd_refine_syev", n, pa, lda, _ptr(w), px, ldx, iters, _ptr(work), nw, _stream(stream))
+    return w, X
 
 
 def stebz(d: torch.Tensor, e: torch.Tensor, stream=None) -> torch.Tensor:

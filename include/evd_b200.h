@@ -263,6 +263,20 @@ int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, dou
 int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
                      long lwork_bytes, int timed, cudaStream_t stream);
 
+/* ---- Iterative refinement of eigenpairs -------------------------------- */
+
+/* No counterpart in the reference.  Ogita-Aishima refinement (RefSyEv,
+ * JJIAM 35 (2018), Algorithm 1) of approximate eigenpairs of the symmetric A:
+ * each iteration forms R = I - X^T X and S = X^T A X with FP64 DMMA GEMMs,
+ * l_i = s_ii / (1 - r_ii), the correction E (clustered pairs, |l_i - l_j| <=
+ * delta, get r_ij / 2) and X <- X + X E; w receives the l_i of the last
+ * iteration (in the column order of X).  The error of X falls quadratically
+ * while it is well below the eigenvalue gaps; 8 n^3 flops per iteration.
+ * n <= 65535; work: evd_refine_syev_work_size(n) doubles (3 n^2 + O(n)). */
+long evd_refine_syev_work_size(long n);
+int evd_refine_syev(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
+                    double* work, long lwork, cudaStream_t stream);
+
 /* ---- FP32 / FP16 entry points of the reference's API -------------------- */
 
 /* The reference instantiates panelQR and tc_ozimmu_syr2k for float and half
