@@ -202,11 +202,7 @@ def run_ours(args) -> int:
     # taken before the solver warms the GPU up
     fp64_peak = max(evd.fp64_peak_tflops() for _ in range(3))
     with torch.cuda.stream(stream):
-        g = torch.Generator(device=dev).manual_seed(1234 + rank)
-        G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
-        A = evd.empty_cm(n, n, device=dev)
-        A.copy_(0.5 * (G + G.t()))
-        del G
+        A, lam_known = _make_input(args.input, n, dev, 1234 + rank)
         ws = evd.Workspace(n, b, nb, device=dev)
         w = torch.empty(n, dtype=torch.float64, device=dev)
         X = evd.empty_cm(n, n, device=dev)
@@ -247,6 +243,9 @@ def run_ours(args) -> int:
     # ---- accuracy of the last result ----
     with torch.cuda.stream(stream):
         resid, orth = evd.check_eig(A, w, X, stream=stream)
+    eig_err = None
+    if lam_known is not None:  # against the spectrum the input was built from
+        eig_err = float((w - lam_known).abs().max() / lam_known.abs().max())
 
     # ---- e2e through the public API with host buffers ----
     A_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
@@ -307,13 +306,14 @@ def run_ours(args) -> int:
         "metric": METRIC, "value": ms_max / 1000.0 / world, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic: seeded symmetrised Gaussian A=(G+G^T)/2 (torch Philox seed 1234+rank)",
+        "data": INPUT_DESC[args.input] + " (torch Philox seed 1234+rank)",
         "config": {"workload": f"plain FP64 two-stage EVD n={n} b={b} nb={nb}", "n": n, "b": b,
+                   "input": args.input,
                    "nb": nb, "parallelism": f"replicas x{world}",
                    "l2": "inputs 2 GiB > 126 MB L2 (no flush needed)"},
         "stages_ms": {k: round(v, 3) for k, v in stages.items()},
         "accuracy": {"resid": resid, "orth": orth, "resid_ok": resid <= 1e-13,
-                     "orth_ok": orth <= 1e-13},
+                     "orth_ok": orth <= 1e-13, "eig_err_vs_known_rel": eig_err},
         "e2e": {"value": e2e_ms / 1000.0 / world, "unit": UNIT,
                 "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * 8 + n * n * 8},
         "gpu_launches": launches_per_step * args.steps,
@@ -325,6 +325,55 @@ def run_ours(args) -> int:
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+INPUT_DESC = {
+    "gauss": "synthetic: seeded symmetrised Gaussian A=(G+G^T)/2",
+    "geometric": "synthetic: A = Q diag(lambda) Q^T, Q Haar (QR of a seeded Gaussian, sign(diag R) "
+                 "fixed), |lambda| geometric over [1e-6, 1] with seeded random signs",
+    "geometric1e10": "synthetic: A = Q diag(lambda) Q^T, Q Haar, |lambda| geometric over "
+                     "[1e-10, 1] with seeded random signs",
+    "uniform": "synthetic: A = Q diag(lambda) Q^T, Q Haar, lambda uniform on [-1, 1]",
+    "clustered": "synthetic: A = Q diag(lambda) Q^T, Q Haar, 100 clusters of width 1e-10 centred "
+                 "on linspace(-1, 1, 100)",
+}
+
+
+def _make_input(kind: str, n: int, dev, seed: int):
+    """(A column-major FP64 on dev, known ascending spectrum or None)."""
+    import torch
+
+    import evd4sc2025_b200 as evd
+
+    g = torch.Generator(device=dev).manual_seed(seed)
+    A = evd.empty_cm(n, n, device=dev)
+    if kind == "gauss":
+        G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
+        A.copy_(0.5 * (G + G.t()))
+        return A, None
+    if kind in ("geometric", "geometric1e10"):
+        decades = 6.0 if kind == "geometric" else 10.0
+        mag = 10.0 ** (-decades * torch.arange(n, dtype=torch.float64, device=dev) / max(n - 1, 1))
+        sign = torch.where(torch.rand(n, generator=g, dtype=torch.float64, device=dev) < 0.5,
+                           -1.0, 1.0)
+        lam = mag * sign
+    elif kind == "uniform":
+        lam = 2.0 * torch.rand(n, generator=g, dtype=torch.float64, device=dev) - 1.0
+    elif kind == "clustered":
+        per = -(-n // 100)
+        centers = torch.linspace(-1.0, 1.0, 100, dtype=torch.float64, device=dev)
+        lam = (centers[:, None] + 1e-10 * torch.rand(100, per, generator=g, dtype=torch.float64,
+                                                     device=dev)).reshape(-1)[:n]
+    else:
+        raise ValueError(kind)
+    G = torch.randn(n, n, generator=g, dtype=torch.float64, device=dev)
+    Q, R = torch.linalg.qr(G)
+    Q *= torch.sign(torch.diagonal(R))[None, :]
+    del G, R
+    M = (Q * lam[None, :]) @ Q.t()
+    A.copy_(0.5 * (M + M.t()))
+    del M, Q
+    return A, torch.sort(lam).values
 
 
 def _loguniform_sizes(count: int, lo: int, hi: int, seed: int) -> list[int]:
@@ -458,6 +507,8 @@ def main(argv=None) -> int:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=16384)
     ap.add_argument("--nb", type=int, default=1024)
+    ap.add_argument("--input", choices=tuple(INPUT_DESC), default="gauss",
+                    help="evd workload input: gauss (default) or a known spectrum")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU LAPACK baseline")
     ap.add_argument("--workload", choices=("evd", "values", "batched", "serving"), default="evd",
                     help="evd (default): the n=16384 solve; batched / serving: the uneven-size "
