@@ -114,6 +114,39 @@ __device__ __forceinline__ void tile_store(double* sub, const double* t, long c0
   for (int i = threadIdx.x; i < n2; i += kChaseThreads) __stcg(dst + i, src[i]);
 }
 
+// Reductions on the tensor pipe.  Inside a chase step the warp shuffles queue
+// behind the shared-memory traffic of the tile copies (a 5-level shuffle sum
+// took about 2400 cycles there, 190 alone); the DMMA unit is otherwise idle.
+// mma.m8n8k4.f64 fragments: lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma884(double& d0, double& d1, double a, double b) {
+  asm volatile(
+      "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%4,%5};\n"
+      : "=d"(d0), "=d"(d1)
+      : "d"(a), "d"(b), "d"(0.0), "d"(0.0));
+}
+
+// Sum over each quad of lanes (4i .. 4i+3): A = values, B = ones.
+__device__ __forceinline__ double quad_sum_tc(double v) {
+  double d0, d1;
+  dmma884(d0, d1, v, 1.0);
+  return d0;
+}
+
+// Sum over the warp, returned to every lane: quad sums s_i (A = values,
+// B = ones); then B2[0][j] = s_j gives D = s_j per column, so lane l holds
+// s_{2(l%4)} and s_{2(l%4)+1}; their sum u_{l%4} as A3[i][k] = u_k against
+// ones adds the four u_k.
+__device__ __forceinline__ double warp_sum_tc(double v) {
+  const int lane = threadIdx.x & 31;
+  double d0, d1;
+  dmma884(d0, d1, v, 1.0);
+  dmma884(d0, d1, 1.0, (lane & 3) == 0 ? d0 : 0.0);
+  const double u = d0 + d1;
+  dmma884(d0, d1, u, 1.0);
+  return d0;
+}
+
 struct ChaseSmem {
   double tile[2][kTileD];  // band columns [base, base+32), element (c, o) at c*64 + o
   double u[kBW];
@@ -165,7 +198,7 @@ __global__ void __launch_bounds__(kChaseThreads)
       // (2) Householder vector from B1[:, 0] = P[0][cb + i]
       if (warp == 0) {
         const double x = (lane < rb) ? P[cb + lane] : 0.0;
-        const double nrm2 = warp_sum(x * x);
+        const double nrm2 = warp_sum_tc(x * x);
         double u = 0.0;
         if (nrm2 > 0.0) {
           u = x * rsqrt(nrm2);
@@ -190,8 +223,7 @@ __global__ void __launch_bounds__(kChaseThreads)
             pv = fma(sm.u[i], P[j * kOff + cb + i - j], pv);
           }
         }
-        pv += __shfl_xor_sync(0xffffffffu, pv, 1);
-        pv += __shfl_xor_sync(0xffffffffu, pv, 2);
+        pv = quad_sum_tc(pv);
         if (j < cb) {
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
@@ -225,11 +257,10 @@ __global__ void __launch_bounds__(kChaseThreads)
           const double sv = (j <= i) ? T[j * kOff + (i - j)] : T[i * kOff + (j - i)];
           y = fma(sv, sm.u[j], y);
         }
-        y += __shfl_xor_sync(0xffffffffu, y, 1);
-        y += __shfl_xor_sync(0xffffffffu, y, 2);
+        y = quad_sum_tc(y);
         // t = u^T y over the 32 rows: rows 8w..8w+7 live in warp w (p == 0 lanes)
         double uy = (p == 0) ? sm.u[i] * y : 0.0;
-        uy = warp_sum(uy);
+        uy = warp_sum_tc(uy);
         if (lane == 0) sm.red[warp] = uy;
         __syncthreads();
         const double t = (sm.red[0] + sm.red[1]) + (sm.red[2] + sm.red[3]);
@@ -253,8 +284,7 @@ __global__ void __launch_bounds__(kChaseThreads)
           const int j = 8 * p + k;
           if (j < rb) w = fma(T[j * kOff + rb + i - j], sm.u[j], w);
         }
-        w += __shfl_xor_sync(0xffffffffu, w, 1);
-        w += __shfl_xor_sync(0xffffffffu, w, 2);
+        w = quad_sum_tc(w);
         if (i < rb2) {
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
