@@ -480,9 +480,14 @@ def run_serving(args) -> int:
     torch.cuda.set_device(dev)
     reqs = serve.poisson_stream(args.requests, args.rate, 128, 8192, seed=2024)
     srv = serve.Server(nworkers=args.streams, budget_bytes=150 * 10**9, device=dev)
-    # warm the workers on a few small requests first (not counted)
-    warm = serve.Server(nworkers=args.streams, budget_bytes=150 * 10**9, device=dev)
-    warm.run(serve.poisson_stream(2 * args.streams, 1e4, 128, 512, seed=1))
+    # warm-up (not counted): every worker grows its buffers to the largest
+    # order of the stream and every kernel is loaded once
+    g = torch.Generator().manual_seed(5)
+    warm = []
+    for i, n in enumerate([8192] * args.streams + [128, 512, 2048] * 2):
+        G = torch.randn(n, n, generator=g, dtype=torch.float64)
+        warm.append(serve.Request(0.0, i, 0.5 * (G + G.t())))
+    srv.run(warm)
     stats = srv.run(reqs)
     lat = [r.latency for r in srv.results]
     line = {"metric": "serving solves/s with p50/p99 latency (FP64 accuracy)",

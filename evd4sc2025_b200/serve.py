@@ -265,7 +265,15 @@ class Server:
                 self._cv.notify_all()
 
     def run(self, requests: list[Request]) -> dict:
-        """Serve the stream; returns throughput and latency statistics."""
+        """Serve the stream; returns throughput and latency statistics.  A
+        server can run several streams one after another (the workers keep
+        their grown buffers); results and statistics are per run."""
+        with self._cv:
+            self._closed = False
+            self._results = []
+            self._ready = []
+            self._in_use = 0
+            self.max_in_flight_bytes = 0
         reqs = sorted(requests)
         for r in reqs:
             r.bytes = int(self.footprint_fn(r.A.shape[0]))

@@ -124,3 +124,14 @@ def test_autotune_active_table_switch():
         assert autotune.choose_nb(512) is None and serve.solve_shape(512) == serve.padded_shape(512)
     finally:
         autotune._cached = autotune._cached_path = None
+
+
+def test_server_runs_twice():
+    """A server can serve a second stream after the first (warm-up, then the
+    measured stream); results and statistics are per run."""
+    srv = serve.Server(nworkers=2, budget_bytes=100, solve_fn=lambda k, A: (A, A),
+                       footprint_fn=lambda n: n)
+    first = srv.run(_fake_requests([3, 4, 5], gap=0.0))
+    assert first["requests"] == 3
+    second = srv.run(_fake_requests([6, 7], gap=0.0))
+    assert second["requests"] == 2 and len(srv.results) == 2
