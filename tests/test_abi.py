@@ -64,6 +64,16 @@ def test_workspace_queries(evdlib):
     ("evd_bc_back", (None, 10, None, 10, 10, 16, None)),
     ("evd_syevd", (1000, 32, 1024, None, 1000, None, None, 1000, None, 0, 0, None)),
     ("evd_dgemm", (b"n", b"n", 10, 10, 10, 1.0, None, 5, None, 10, 0.0, None, 10, None)),
+    ("evd_syevd_values", (1000, 32, 1024, None, 1000, None, None, 0, 0, None)),
+    ("evd_refine_syev", (10, None, 10, None, None, 10, 2, None, 0, None)),
+    ("evd_refine_syev", (70000, 256, 70000, 256, 256, 70000, 1, 256, 1 << 40, None)),
+    ("evd_tc_syr2k", (10, 4, 1.0, 256, 5, 256, 10, 0.0, 256, 10, None, 0, None)),   # lda < n
+    ("evd_syr2k_lower_s", (10, 4, 1.0, 256, 10, 256, 10, 0.0, 256, 5, 0, None)),    # ldc < n
+    ("evd_syr2k_lower_h", (10, 4, 1.0, None, 10, 256, 10, 0.0, 256, 10, 0, None)),  # A missing
+    ("evd_panel_qr_s", (100, 32, None, 100, None, 100, None, 32, None, 0, None)),
+    ("evd_tsqr_h", (64, 16, None, 64, None, 32, None, 0, None)),
+    ("evd_stebz", (-1, None, None, None, None, 100, None)),
+    ("evd_write_matrix_bin", (None, 0, 2, 2, None, 2)),
 ])
 def test_invalid_arguments_rejected_without_gpu(evdlib, call, args):
     # every check happens on the host before any CUDA call
@@ -74,3 +84,14 @@ def test_invalid_arguments_rejected_without_gpu(evdlib, call, args):
 def test_oracle_not_imported_by_product():
     src = "\n".join(p.read_text() for p in (ROOT / "evd4sc2025_b200").rglob("*.py"))
     assert "oracle" not in src.replace("no fallback", "")  # the product never touches oracle/
+
+
+def test_workspace_too_small_reported_without_gpu(evdlib):
+    lib = evdlib.lib()
+    # non-null placeholders are never dereferenced: the size check comes first
+    assert lib.evd_refine_syev(8, 256, 8, 256, 256, 8, 1, 256, 10, None) == -5
+    assert lib.evd_refine_syev_work_size(8) > 3 * 64
+    assert lib.evd_refine_syev_work_size(70000) == 0
+    assert lib.evd_panel_qr_lp_work_size(4096, 32) > 8 * 2 * 4096 * 32
+    assert lib.evd_panel_qr_lp_work_size(4096, 16) == 0
+    assert lib.evd_panel_qr_s(128, 32, 256, 128, 256, 128, 256, 32, 256, 10, None) == -5
