@@ -254,11 +254,11 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
   }
 }
 
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  // start >> 4 | LBO (128 B) >> 4 << 16 | SBO (1024 B) >> 4 << 32 | version 1 << 46;
-  // base offset 0, no swizzle
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo = 1024) {
+  // start >> 4 | LBO (128 B, K direction) >> 4 << 16 | SBO (row-group stride) >> 4 << 32 |
+  // version 1 << 46; base offset 0, no swizzle
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
-         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46);
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
 // kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B F16 (0),
@@ -420,8 +420,11 @@ __global__ void __launch_bounds__(kTThreads) tc_syr2k_kernel(long n, long k, flo
 // H[m][kk] = A(m, kk), H[m][k8 + kk] = B(m, kk), zero in the padding.  Rows of
 // H are the K-major rows the tensor core reads, so a stage is filled by
 // 16-byte cp.async copies straight into the core-matrix layout.
+// 16-byte copy through L1 (.ca): two threads share each 32-byte sector, and
+// the L1-allocating form moved about 13 % more operand bytes per second than
+// .cg in the tensor-core kernel below.
 __device__ __forceinline__ void cp_async16z(void* smem, const void* gmem, int src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)),
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)),
                "l"(gmem), "r"(src_bytes)
                : "memory");
 }
@@ -451,24 +454,64 @@ __global__ void pack_h_kernel(long n, long k, long k8, const TI* __restrict__ A,
   }
 }
 
+// The tensor-core kernel for packed operands: warps 0-3 copy (16-byte
+// cp.async, K chunks of 64 through 3 stages, 2 chunks in flight per thread),
+// warp 4 issues the MMAs.  Operand tiles use the 128-byte-swizzled K-major
+// layout: row r of a tile is 128 contiguous bytes (64 halves of K) at
+// (r / 8) * 1024 + (r % 8) * 128, its 16-byte chunk c stored at chunk
+// c ^ (r % 8), tiles 1024-byte aligned; the descriptor says SWIZZLE_128B with
+// a 1024-byte stride between 8-row groups, and the K16 steps inside a chunk
+// advance the start address by 32 bytes.  A producer completes its own copies
+// of a chunk (wait_group), makes them visible to the tensor core
+// (fence.proxy.async) and arrives on the chunk's `full` barrier (128
+// arrivals); the MMA warp waits on `full`, issues four K16 MMAs and commits
+// them to the stage's `empty` barrier, which the producers wait on before
+// refilling the stage.  No block-wide barrier in the main loop; every wait is
+// bounded.
+constexpr int kWK = 64, kWS = 3, kWD = kWS - 1;      // K chunk, stages, chunks in flight
+constexpr int kWTile = kTM * kWK * 2;                // 16 KB per operand tile
+constexpr int kWStage = 2 * kWTile;
+constexpr int kWProd = 128, kWThreads = kWProd + 32;
+constexpr int kWSmem = kWS * kWStage + 1024 + 256;   // + alignment slack, barriers
+
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  // start >> 4 | LBO 16 B (unused for swizzled K-major) | SBO 1024 B | version 1 |
+  // base offset 0 (tiles 1024-aligned, K steps stay inside a 128-byte row) |
+  // layout SWIZZLE_128B (2)
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
 template <typename TC>
-__global__ void __launch_bounds__(kTThreads) tc_syr2k_cp_kernel(long n, long k8, float alpha,
+__global__ void __launch_bounds__(kWThreads) tc_syr2k_ws_kernel(long n, long k8, float alpha,
                                                                 const __half* __restrict__ H,
                                                                 float beta, TC* __restrict__ C,
                                                                 long ldc, int* err) {
   extern __shared__ __align__(1024) uint8_t tsm[];
-  uint8_t* stages = tsm;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tsm + kTStages * kTStageBytes);  // kTStages + 1
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kTStages + 1);
+  // 1024-byte aligned tile area (the swizzle pattern repeats every 1024 bytes)
+  uint8_t* stages = tsm + ((1024u - (smem_u32(tsm) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kWS * kWStage);
+  uint64_t* empty = full + kWS;
+  uint64_t* done = empty + kWS;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   long bi, bj;
   tri_tile(blockIdx.x, bi, bj);
   const long m0 = bi * kTM, n0 = bj * kTN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long L = 2 * k8;
-  const long nch = (L + kTK - 1) / kTK;
+  const long nch = (L + kWK - 1) / kWK;
 
   if (tid == 0) {
-    for (int s = 0; s <= kTStages; ++s) mbar_init(bars + s, 1);
+    for (int s = 0; s < kWS; ++s) {
+      mbar_init(full + s, kWProd);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -483,66 +526,74 @@ __global__ void __launch_bounds__(kTThreads) tc_syr2k_cp_kernel(long n, long k8,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
 
-  // chunk t: left rows m0.. at K offset 64 t of H ([A | B]); right rows n0.. at
-  // K offset 64 t + k8 (mod L) of H ([B | A]).  Thread t copies 8 segments of
-  // 16 bytes per operand: segment q = tid + 128 i -> row q >> 3, K core q & 7.
-  auto issue = [&](long t, int s) {
-    uint8_t* Lt = stages + s * kTStageBytes;
-    uint8_t* Rt = Lt + kTTileBytes;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int q = tid + i * kTThreads;
-      const int row = q >> 3, c = q & 7;
-      const int off = ((row >> 3) * 8 + c) * 128 + (row & 7) * 16;
-      const long kk = t * kTK + c * 8;
-      const bool kv = kk < L;
-      long kr = kk + k8;
-      if (kr >= L) kr -= L;
-      const long gl = m0 + row, gr = n0 + row;
-      const bool lv = kv && gl < n, rv = kv && gr < n;
-      cp_async16z(Lt + off, lv ? (const void*)(H + gl * L + kk) : (const void*)H, lv ? 16 : 0);
-      cp_async16z(Rt + off, rv ? (const void*)(H + gr * L + kr) : (const void*)H, rv ? 16 : 0);
-    }
-  };
-
-  for (int t = 0; t < kTStages - 1; ++t) {
-    if (t < nch) issue(t, t);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-  }
   bool ok = true;
-  for (long t = 0; t < nch; ++t) {
-    const int s = (int)(t % kTStages);
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(kTStages - 2) : "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t la = smem_u32(stages + s * kTStageBytes), ra = la + kTTileBytes;
+  if (warp < 4) {
+    // ---- producers: chunk t -> stage t % kWS ----
+    auto issue = [&](long t, int s) {
+      uint8_t* Lt = stages + s * kWStage;
+      uint8_t* Rt = Lt + kWTile;
 #pragma unroll
-      for (int ks = 0; ks < kTK / 16; ++ks)
-        umma_f16(tmem, smem_desc(la + ks * 256), smem_desc(ra + ks * 256),
-                 (t > 0 || ks > 0) ? 1u : 0u);
-      umma_commit(bars + s);
-    }
-    // refill: chunk t + S - 1 goes into the stage chunk t - 1 used
-    const long tn = t + kTStages - 1;
-    if (tn < nch) {
-      if (t >= 1) {
-        const long tp = t - 1;
-        ok = mbar_wait(bars + (int)(tp % kTStages), (uint32_t)((tp / kTStages) & 1), err);
+      for (int i = 0; i < 8; ++i) {
+        const int q = tid + i * kWProd;
+        const int row = q >> 3, c = q & 7;  // 8 threads per 128-byte row: coalesced
+        const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c ^ (row & 7)) << 4);
+        const long kk = t * kWK + c * 8;
+        const bool kv = kk < L;
+        long kr = kk + k8;
+        if (kr >= L) kr -= L;
+        const long gl = m0 + row, gr = n0 + row;
+        const bool lv = kv && gl < n, rv = kv && gr < n;
+        cp_async16z(Lt + off, lv ? (const void*)(H + gl * L + kk) : (const void*)H, lv ? 16 : 0);
+        cp_async16z(Rt + off, rv ? (const void*)(H + gr * L + kr) : (const void*)H, rv ? 16 : 0);
       }
-      ok = __syncthreads_and(ok);
-      if (!ok) break;
-      issue(tn, (int)(tn % kTStages));
+    };
+    long arrived = 0;  // chunks whose `full` barrier this thread has arrived on
+    for (long t = 0; t < nch; ++t) {
+      const int s = (int)(t % kWS);
+      if (t >= kWS && !mbar_wait(empty + s, (uint32_t)((t / kWS - 1) & 1), err)) {
+        ok = false;
+        break;
+      }
+      issue(t, s);
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      if (t >= kWD - 1) {  // chunk t - (kWD - 1) has landed
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kWD - 1) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(full + (int)(arrived % kWS));
+        ++arrived;
+      }
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (ok)
+      for (; arrived < nch; ++arrived) mbar_arrive(full + (int)(arrived % kWS));
+  } else {
+    // ---- MMA warp: lane 0 issues, the whole warp waits ----
+    for (long t = 0; t < nch; ++t) {
+      const int s = (int)(t % kWS);
+      if (!mbar_wait(full + s, (uint32_t)((t / kWS) & 1), err)) {
+        ok = false;
+        break;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t la = smem_u32(stages + s * kWStage), ra = la + kWTile;
+#pragma unroll
+        for (int ks = 0; ks < kWK / 16; ++ks)
+          umma_f16(tmem, smem_desc_sw128(la + ks * 32), smem_desc_sw128(ra + ks * 32),
+                   (t > 0 || ks > 0) ? 1u : 0u);
+        umma_commit(empty + s);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) umma_commit(done);  // all MMAs issued above complete -> done
+    __syncwarp();
   }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-  if (tid == 0) umma_commit(bars + kTStages);
-  const bool done = mbar_wait(bars + kTStages, 0, err);
-  ok = __syncthreads_and(ok && done);
+  const bool fin = mbar_wait(done, 0, err);
+  ok = __syncthreads_and(ok && fin);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
+  if (ok && warp < 4) {
     const long gi = m0 + warp * 32 + lane;
 #pragma unroll 1
     for (int c0 = 0; c0 < kTN; c0 += 16) {
@@ -572,7 +623,7 @@ __global__ void __launch_bounds__(kTThreads) tc_syr2k_cp_kernel(long n, long k8,
                  : "memory");
 }
 
-// A, B -> H in `hwork` (n x 2 k8 halves), then the cp.async-fed kernel.
+// A, B -> H in `hwork` (n x 2 k8 halves), then the warp-specialised kernel.
 template <typename TI, typename TC>
 int tc_syr2k_packed(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
                     float beta, TC* C, long ldc, __half* H, int* err, cudaStream_t st) {
@@ -582,9 +633,9 @@ int tc_syr2k_packed(long n, long k, float alpha, const TI* A, long lda, const TI
   pack_h_kernel<TI><<<pg, dim3(32, 8), 0, st>>>(n, k, k8, A, lda, B, ldb, H);
   EVD_LAUNCHED();
   const long T = (n + kTM - 1) / kTM;
-  EVD_CUDA_TRY(cudaFuncSetAttribute(tc_syr2k_cp_kernel<TC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kTSmem));
-  tc_syr2k_cp_kernel<TC><<<(unsigned)(T * (T + 1) / 2), kTThreads, kTSmem, st>>>(
+  EVD_CUDA_TRY(cudaFuncSetAttribute(tc_syr2k_ws_kernel<TC>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem));
+  tc_syr2k_ws_kernel<TC><<<(unsigned)(T * (T + 1) / 2), kWThreads, kWSmem, st>>>(
       n, k8, alpha, H, beta, C, ldc, err);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
