@@ -7,12 +7,13 @@
 // The B200 versions:
 //
 // * tc_syr2k and the half SYR2K run one tcgen05 kernel: both operands are
-//   rounded to FP16 while they are staged into shared memory (so the FP16
-//   copy the reference makes in `hwork` first is not needed), each 64-wide K
-//   chunk is multiplied by `tcgen05.mma.kind::f16` into a 128 x 128 FP32
-//   accumulator in tensor memory, and the epilogue applies alpha / beta on
-//   the lower triangle.  A B^T + B A^T is one product over the concatenated
-//   K range: [A | B] * [B | A]^T.
+//   packed once as FP16 rows with K contiguous (into the reference's `hwork`
+//   when it fits, else a stream-ordered buffer), streamed into 128-byte-
+//   swizzled shared-memory tiles by copy warps, multiplied 64 K at a time by
+//   `tcgen05.mma.kind::f16` into a 128 x 128 FP32 accumulator in tensor
+//   memory, and the epilogue applies alpha / beta on the lower triangle.
+//   A B^T + B A^T is one product over the concatenated K range:
+//   [A | B] * [B | A]^T.
 // * the FP32 SYR2K is a SIMT FP32 kernel (exact FP32 multiply-add, the
 //   arithmetic of CUBLAS_COMPUTE_32F that the reference asks cuBLAS for).
 // * the FP32 / FP16 panel QR and TSQR convert the panel to FP64, run the
@@ -201,17 +202,10 @@ __global__ void __launch_bounds__(256) ssyr2k_kernel(long n, long k, float alpha
 }
 
 // ------------------------------------------------ tcgen05 FP16 SYR2K (TMEM)
-// Tile 128 x 128 of C per CTA (128 threads), K chunks of 64 staged as FP16 in
-// the canonical K-major layout without swizzle: core matrices of 8 rows x 16
-// bytes (128 contiguous bytes), core (row group g, K core c) at
-// (g * 8 + c) * 128 bytes, so the leading (K) byte offset is 128 and the
-// stride (row-group) byte offset is 1024.  One elected thread issues four
-// M128 N128 K16 MMAs per chunk and commits them to the chunk's mbarrier;
-// three stages let the staging of chunk t+1, t+2 overlap the MMAs of chunk t.
-constexpr int kTM = 128, kTN = 128, kTK = 64, kTStages = 3, kTThreads = 128;
-constexpr int kTTileBytes = kTM * kTK * 2;          // 16 KB per operand tile
-constexpr int kTStageBytes = 2 * kTTileBytes;        // left + right
-constexpr int kTSmem = kTStages * kTStageBytes + 256;  // + barriers, TMEM slot, alignment
+// Tile 128 x 128 of C per CTA; the operands are packed once into FP16 rows
+// with K contiguous (below), then streamed into shared memory and multiplied
+// by tcgen05.mma into an FP32 accumulator in tensor memory.
+constexpr int kTM = 128, kTN = 128;
 constexpr unsigned long long kTWaitNs = 2000000000ull;  // 2 s per wait: far above any chunk
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -254,12 +248,6 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
   }
 }
 
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo = 1024) {
-  // start >> 4 | LBO (128 B, K direction) >> 4 << 16 | SBO (row-group stride) >> 4 << 32 |
-  // version 1 << 46; base offset 0, no swizzle
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
 
 // kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B F16 (0),
 // both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
@@ -283,136 +271,11 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_elem(const __half* p) { return __half2float(p[0]); }
 
-// Stage rows [r0, r0 + 128) x K-chunk [kk0, kk0 + 64) of P (n x k) as FP16
-// into `tile` (K-major canonical layout), zero beyond row n and column k.
-// Thread t owns row t: 8 K cores of 8 values, each one 16-byte core row.
-template <typename T>
-__device__ __forceinline__ void stage_rows(uint8_t* tile, const T* __restrict__ P, long ldp, long n,
-                                           long k, long r0, long kk0) {
-  const int t = threadIdx.x;
-  const long r = r0 + t;
-  const bool rok = r < n;
-  uint8_t* rowbase = tile + (t >> 3) * 1024 + (t & 7) * 16;
-#pragma unroll 2
-  for (int c = 0; c < 8; ++c) {
-    float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const long kk = kk0 + c * 8 + q;
-      v[q] = (rok && kk < k) ? ld_elem(P + r + kk * ldp) : 0.0f;
-    }
-    __half2 h[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) h[q] = __floats2half2_rn(v[2 * q], v[2 * q + 1]);
-    *reinterpret_cast<uint4*>(rowbase + c * 128) = *reinterpret_cast<const uint4*>(h);
-  }
-}
-
 __device__ __forceinline__ void store_c(float* c, float v, float alpha, float beta) {
   *c = (beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * *c);
 }
 __device__ __forceinline__ void store_c(__half* c, float v, float alpha, float beta) {
   *c = __float2half_rn((beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * __half2float(*c)));
-}
-
-template <typename TI, typename TC>
-__global__ void __launch_bounds__(kTThreads) tc_syr2k_kernel(long n, long k, float alpha,
-                                                             const TI* __restrict__ A, long lda,
-                                                             const TI* __restrict__ B, long ldb,
-                                                             float beta, TC* __restrict__ C,
-                                                             long ldc, int* err) {
-  extern __shared__ __align__(1024) uint8_t tsm[];
-  uint8_t* stages = tsm;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tsm + kTStages * kTStageBytes);  // kTStages + 1
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kTStages + 1);
-  long bi, bj;
-  tri_tile(blockIdx.x, bi, bj);
-  const long m0 = bi * kTM, n0 = bj * kTN;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-  if (tid == 0) {
-    for (int s = 0; s <= kTStages; ++s) mbar_init(bars + s, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(tslot)),
-                 "r"(kTN)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tmem = *tslot;
-
-  const long kc = (k + kTK - 1) / kTK;  // chunks per half of [A | B]
-  const long nch = 2 * kc;
-  bool ok = true;
-  for (long t = 0; t < nch && ok; ++t) {
-    const int s = (int)(t % kTStages);
-    uint8_t* Lt = stages + s * kTStageBytes;
-    uint8_t* Rt = Lt + kTTileBytes;
-    if (t >= kTStages) ok = mbar_wait(bars + s, (uint32_t)((t / kTStages - 1) & 1), err);
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    // chunk t of the concatenated K range: the first kc chunks come from
-    // (A, B), the last kc from (B, A); each half is zero-padded to kc * 64
-    const long kk0 = (t < kc) ? t * kTK : (t - kc) * kTK;
-    if (t < kc) {
-      stage_rows(Lt, A, lda, n, k, m0, kk0);
-      stage_rows(Rt, B, ldb, n, k, n0, kk0);
-    } else {
-      stage_rows(Lt, B, ldb, n, k, m0, kk0);
-      stage_rows(Rt, A, lda, n, k, n0, kk0);
-    }
-    // make the generic-proxy shared stores visible to the tensor core
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t la = smem_u32(Lt), ra = smem_u32(Rt);
-#pragma unroll
-      for (int ks = 0; ks < kTK / 16; ++ks)
-        umma_f16(tmem, smem_desc(la + ks * 256), smem_desc(ra + ks * 256),
-                 (t > 0 || ks > 0) ? 1u : 0u);
-      umma_commit(bars + s);
-    }
-  }
-  // all MMAs issued by thread 0 complete -> the done barrier
-  if (tid == 0) umma_commit(bars + kTStages);
-  const bool done = mbar_wait(bars + kTStages, 0, err);
-  ok = __syncthreads_and(ok && done);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
-    // epilogue: warp w reads TMEM lanes 32w .. 32w + 31 (rows of the tile)
-    const long gi = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < kTN; c0 += 16) {
-      uint32_t v[16];
-      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-          "%11, %12, %13, %14, %15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (gi < n) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const long gj = n0 + c0 + j;
-          if (gj <= gi) store_c(C + gi + gj * ldc, __uint_as_float(v[j]), alpha, beta);
-        }
-      }
-    }
-  }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTN)
-                 : "memory");
 }
 
 // ---- FP16 operand copy + cp.async-fed tensor-core SYR2K ----
@@ -641,19 +504,6 @@ int tc_syr2k_packed(long n, long k, float alpha, const TI* A, long lda, const TI
   return EVD_SUCCESS;
 }
 
-template <typename TI, typename TC>
-int tc_syr2k_launch(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
-                    float beta, TC* C, long ldc, int* err, cudaStream_t st) {
-  const long T = (n + kTM - 1) / kTM;
-  const long tiles = T * (T + 1) / 2;
-  EVD_CUDA_TRY(cudaFuncSetAttribute(tc_syr2k_kernel<TI, TC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kTSmem));
-  tc_syr2k_kernel<TI, TC><<<(unsigned)tiles, kTThreads, kTSmem, st>>>(n, k, alpha, A, lda, B, ldb,
-                                                                     beta, C, ldc, err);
-  EVD_LAUNCHED();
-  return EVD_SUCCESS;
-}
-
 bool syr2k_args_ok(long n, long k, const void* A, long lda, const void* B, long ldb,
                    const void* C, long ldc) {
   if (n < 0 || k < 0 || ldc < std::max(1L, n)) return false;
@@ -705,6 +555,55 @@ int check_tc_err(int* err, cudaStream_t st) {
     return EVD_ERR_TIMEOUT;
   }
   return EVD_SUCCESS;
+}
+
+// Library-private stream-ordered memory pool of the current device: it keeps
+// its memory between calls (no release threshold), so a repeated call does
+// not pay for a fresh allocation; the application's default pool is left as
+// it is.
+cudaMemPool_t lp_pool() {
+  static cudaMemPool_t pools[64] = {nullptr};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+  if (!pools[d]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = d;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    if (cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+      return nullptr;
+    pools[d] = p;
+  }
+  return pools[d];
+}
+
+// Packs A, B into H (the caller's workspace, or a buffer of n x 2 k8 halves
+// from the library's pool when H is null), runs the tensor-core kernel and
+// reads the kernel's error word.
+template <typename TI, typename TC>
+int tc_syr2k_run(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
+                 float beta, TC* C, long ldc, __half* H, cudaStream_t st) {
+  const long k8 = (k + 7) / 8 * 8;
+  if ((2 * k8 + 31) / 32 >= 65536 || (n + 31) / 32 >= (1L << 31)) return EVD_ERR_INVALID_ARG;
+  int* err = tc_err_word();
+  if (!err) return EVD_ERR_CUDA;
+  __half* own = nullptr;
+  if (H == nullptr) {
+    cudaMemPool_t pool = lp_pool();
+    if (!pool) return EVD_ERR_CUDA;
+    EVD_CUDA_TRY(
+        cudaMallocFromPoolAsync((void**)&own, sizeof(__half) * (size_t)n * 2 * k8, pool, st));
+    H = own;
+  }
+  const int rc = tc_syr2k_packed(n, k, alpha, A, lda, B, ldb, beta, C, ldc, H, err, st);
+  if (own) EVD_CUDA_TRY(cudaFreeAsync(own, st));
+  EVD_TRY(rc);
+  return check_tc_err(err, st);
 }
 
 }  // namespace
@@ -761,19 +660,11 @@ extern "C" int evd_tc_syr2k(long n, long k, float alpha, const float* A, long ld
   if (!evd::syr2k_args_ok(n, k, A, lda, B, ldb, C, ldc)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, C, ldc, stream);
-  int* err = evd::tc_err_word();
-  if (!err) return EVD_ERR_CUDA;
-  // with the reference's FP16 workspace (2 n k halves) and k % 8 == 0 the
-  // operands are packed once and streamed by cp.async; otherwise they are
-  // rounded while staged (no workspace needed)
-  const bool packed = hwork != nullptr && k % 8 == 0 && ((uintptr_t)hwork & 15) == 0 &&
-                      (n + 31) / 32 < (1L << 31) && (2 * k + 31) / 32 < 65536;
-  if (packed)
-    EVD_TRY(evd::tc_syr2k_packed(n, k, alpha, A, lda, B, ldb, beta, C, ldc, (__half*)hwork, err,
-                                 stream));
-  else
-    EVD_TRY(evd::tc_syr2k_launch(n, k, alpha, A, lda, B, ldb, beta, C, ldc, err, stream));
-  return evd::check_tc_err(err, stream);
+  // the reference's FP16 workspace (2 n k halves) holds the packed operands
+  // when k % 8 == 0; otherwise (or without one) a stream-ordered buffer does
+  const bool own = hwork == nullptr || k % 8 != 0 || ((uintptr_t)hwork & 15) != 0;
+  return evd::tc_syr2k_run(n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                           own ? nullptr : (__half*)hwork, stream);
 }
 
 extern "C" int evd_syr2k_lower_h(long n, long k, float alpha, const void* A, long lda,
@@ -783,9 +674,6 @@ extern "C" int evd_syr2k_lower_h(long n, long k, float alpha, const void* A, lon
   if (!evd::syr2k_args_ok(n, k, A, lda, B, ldb, C, ldc)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, (__half*)C, ldc, stream);
-  int* err = evd::tc_err_word();
-  if (!err) return EVD_ERR_CUDA;
-  EVD_TRY(evd::tc_syr2k_launch(n, k, alpha, (const __half*)A, lda, (const __half*)B, ldb, beta,
-                               (__half*)C, ldc, err, stream));
-  return evd::check_tc_err(err, stream);
+  return evd::tc_syr2k_run(n, k, alpha, (const __half*)A, lda, (const __half*)B, ldb, beta,
+                           (__half*)C, ldc, nullptr, stream);
 }

@@ -49,7 +49,7 @@ def tc_syr2k(alpha: float, A: torch.Tensor, B: torch.Tensor, beta: float, Cm: to
     """C(lower) = alpha (A B^T + B A^T) + beta C with FP16 products (FP32 data).
 
     ``hwork``: the reference's FP16 workspace (2 n k halves); True allocates
-    it, None runs without one (operands rounded while staged)."""
+    it, None lets the library use a stream-ordered buffer."""
     n, k = A.shape
     pa, lda = _cm(A, "A", (torch.float32,))
     pb, ldb = _cm(B, "B", (torch.float32,))

@@ -303,13 +303,15 @@ int evd_tsqr_h(long m, long n, void* A, long lda, void* R, long ldr, void* work,
 int evd_syr2k_lower_s(long n, long k, float alpha, const float* A, long lda, const float* B,
                       long ldb, float beta, float* C, long ldc, long nb, cudaStream_t stream);
 /* tc_syr2k: as above with A and B rounded to FP16 and the products summed in
- * FP32 on the tcgen05 tensor cores.  The rounding happens while the operands
- * are staged on chip, so `hwork` (the reference's FP16 copy, 2 n k halves) is
- * accepted and not used; nb is accepted and not needed. */
+ * FP32 on the tcgen05 tensor cores.  `hwork` (2 n k halves, as the reference)
+ * receives the packed FP16 operands when k % 8 == 0; with hwork == NULL or
+ * another k the library uses a buffer from its own stream-ordered memory pool.  nb is
+ * accepted and not needed. */
 int evd_tc_syr2k(long n, long k, float alpha, const float* A, long lda, const float* B, long ldb,
                  float beta, float* C, long ldc, void* hwork, long nb, cudaStream_t stream);
 /* tc_ozimmu_syr2k<half>: FP16 A, B, C; FP32 accumulation on the tensor cores
- * (the reference accumulates in FP16, CUBLAS_COMPUTE_16F); alpha, beta as float. */
+ * (the reference accumulates in FP16, CUBLAS_COMPUTE_16F); alpha, beta as float.
+ * Packs the operands into a buffer of 2 n k halves from the library's pool. */
 int evd_syr2k_lower_h(long n, long k, float alpha, const void* A, long lda, const void* B,
                       long ldb, float beta, void* C, long ldc, long nb, cudaStream_t stream);
 
