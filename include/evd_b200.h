@@ -8,6 +8,13 @@
  * No entry point allocates device memory unless its comment says so; the
  * caller passes workspaces sized by the matching *_work_size query.
  *
+ * Synchronisation: entry points whose kernels report through a device error
+ * word (bounded waits, convergence) read it before returning and therefore
+ * synchronise `stream`: evd_bulge_chase(_noalloc), evd_stedc, evd_syevd,
+ * evd_syevd_values, evd_tc_syr2k, evd_syr2k_lower_h, the metrics, the FP64
+ * peak probe and the file functions.  All others only enqueue work on
+ * `stream`.
+ *
  * The comment on each function names the reference interface it replaces
  * (paths relative to the hansheng1001/EVD4SC2025 source tree).  The reference
  * functions take cuBLAS/cuSOLVER handles; this library uses none, so the C++
