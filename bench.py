@@ -442,9 +442,16 @@ def run_batched(args) -> int:
         one = [serve.StreamSolver(dev)]
         serve.syevd_batched(sorted(mats, key=lambda m: -m.shape[0])[:4], solvers=one)
         _, ms_loop = serve.syevd_batched(mats, solvers=one)
+        # the same batch through the C entry point (threads and streams inside
+        # the library; nb by the fixed rule); the matrices are symmetric, so
+        # the transposed views are their column-major forms
+        cms = [m.t() for m in mats]
+        serve.syevd_batched_native(cms, nstreams=args.streams)  # warm-up
+        _, ms_native = serve.syevd_batched_native(cms, nstreams=args.streams)
         flops = sum(16.0 / 3.0 * n ** 3 for n in sizes)
         out.append({"batch": tag, "matrices": count, "n_range": [lo, hi],
                     "solves_per_s": count / (ms * 1e-3), "ms": ms,
+                    "native_c_api_solves_per_s": count / (ms_native * 1e-3),
                     "looped_plain_solves_per_s": count / (ms_loop * 1e-3), "looped_ms": ms_loop,
                     "speedup_vs_loop": ms_loop / ms, "tflops_fp64_equiv": flops / (ms * 1e-3) / 1e12})
     line = {"metric": "batched solves/s (uneven sizes, FP64 accuracy)", "value": out[0]["solves_per_s"],

@@ -55,6 +55,8 @@ SIGNATURES = {
     "evd_stebz": (_i, [_l, _p, _p, _p, _p, _l, _p]),
     "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
+    "evd_syevd_batched_work_size": (_l, [_l, _p, _i]),
+    "evd_syevd_batched": (_i, [_l, _p, _p, _p, _p, _p, _p, _i, _p, _l, _p]),
     "evd_refine_syev_work_size": (_l, [_l]),
     "evd_refine_syev": (_i, [_l, _p, _l, _p, _p, _l, _i, _p, _l, _p]),
     "evd_panel_qr_lp_work_size": (_l, [_l, _l]),

@@ -182,6 +182,45 @@ def syevd_batched(mats: list[torch.Tensor], nstreams: int = 8, device="cuda",
     return out, ms
 
 
+def syevd_batched_native(mats: list[torch.Tensor], nstreams: int = 8, device="cuda",
+                         stream=None):
+    """The same batched solve through the C entry point ``evd_syevd_batched``
+    (host threads and streams inside the library, no Python per solve).
+    ``mats``: column-major FP64 CUDA matrices.  Returns [(w, X), ...] in input
+    order and the device time of the batch in ms."""
+    import ctypes as C
+
+    count = len(mats)
+    dev = torch.device(device)
+    ns = (C.c_long * count)(*[m.shape[0] for m in mats])
+    outs = [(torch.empty(m.shape[0], dtype=F64, device=dev), empty_cm(m.shape[0], m.shape[0],
+                                                                      device=dev)) for m in mats]
+    pa, la, pw, px, lx = [], [], [], [], []
+    for m, (w, X) in zip(mats, outs):
+        p, ld = _cm(m, "A")
+        pa.append(p.value)
+        la.append(ld)
+        pw.append(w.data_ptr())
+        q, ldx = _cm(X, "X")
+        px.append(q.value)
+        lx.append(ldx)
+    nbytes = int(lib().evd_syevd_batched_work_size(count, ns, nstreams))
+    if nbytes <= 0:
+        raise ValueError("unsupported batch")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    arr = lambda t, v: (t * count)(*v)  # noqa: E731
+    st = stream or torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    call("evd_syevd_batched", count, ns, arr(C.c_void_p, pa), arr(C.c_long, la),
+         arr(C.c_void_p, pw), arr(C.c_void_p, px), arr(C.c_long, lx), nstreams,
+         _ptr(ws), nbytes, _stream(st))
+    e1.record(st)
+    e1.synchronize()
+    return outs, e0.elapsed_time(e1)
+
+
 # ------------------------------------------------------------------- serving
 @dataclass(order=True)
 class Request:

@@ -270,6 +270,23 @@ int evd_syevd(long n, long b, long nb, const double* A, long lda, double* w, dou
 int evd_syevd_values(long n, long b, long nb, const double* A, long lda, double* w, void* work,
                      long lwork_bytes, int timed, cudaStream_t stream);
 
+/* ---- Batched solves of uneven orders ------------------------------------ */
+
+/* No counterpart in the reference (one matrix per process, myEVD.cu:251-706).
+ * Eigenpairs of `count` symmetric matrices of any orders n[i] >= 1: A[i]
+ * (n[i] x n[i], lda[i]), w[i] (n[i]), X[i] (n[i] x n[i], ldX[i]), all device
+ * pointers; the pointer and size arrays are HOST arrays.  The solves run on
+ * min(nstreams, count) internal streams (one host thread each, largest
+ * matrices first), after the work already enqueued on `stream`, which waits
+ * for all of them; nb per matrix: the largest 32 * 2^k (<= 1024) dividing
+ * 32 * ceil(n / 32).  work: evd_syevd_batched_work_size bytes (one solver
+ * workspace of the largest order per stream).  nstreams <= 64.  Returns the
+ * first failing solve's status.  Synchronises the internal streams. */
+long evd_syevd_batched_work_size(long count, const long* n, int nstreams);
+int evd_syevd_batched(long count, const long* n, const double* const* A, const long* lda,
+                      double* const* w, double* const* X, const long* ldX, int nstreams,
+                      void* work, long lwork_bytes, cudaStream_t stream);
+
 /* ---- Iterative refinement of eigenpairs -------------------------------- */
 
 /* No counterpart in the reference.  Ogita-Aishima refinement (RefSyEv,

@@ -95,3 +95,14 @@ def test_workspace_too_small_reported_without_gpu(evdlib):
     assert lib.evd_panel_qr_lp_work_size(4096, 32) > 8 * 2 * 4096 * 32
     assert lib.evd_panel_qr_lp_work_size(4096, 16) == 0
     assert lib.evd_panel_qr_s(128, 32, 256, 128, 256, 128, 256, 32, 256, 10, None) == -5
+
+
+def test_batched_queries_without_gpu(evdlib):
+    lib = evdlib.lib()
+    n = (C.c_long * 3)(100, 1000, 64)
+    assert lib.evd_syevd_batched_work_size(3, n, 2) >= 2 * lib.evd_syevd_work_size(1024, 32, 1024)
+    assert lib.evd_syevd_batched_work_size(0, None, 8) > 0
+    assert lib.evd_syevd_batched_work_size(3, n, 0) == 0          # nstreams >= 1
+    bad = (C.c_long * 2)(10, 0)
+    assert lib.evd_syevd_batched_work_size(2, bad, 2) == 0        # order 0
+    assert lib.evd_syevd_batched(2, bad, None, None, None, None, None, 2, None, 0, None) == -1

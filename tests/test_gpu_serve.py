@@ -52,6 +52,22 @@ def test_batched_matches_one_at_a_time(cuda, evdlib):
         _check(A.cpu(), w, X)
 
 
+def test_native_batched_matches_single_solves(cuda, evdlib):
+    """evd_syevd_batched (threads and streams inside the library) gives, for
+    every matrix, exactly what evd_syevd gives alone with the same nb."""
+    sizes = [1, 33, 64, 100, 257, 512, 700, 1024, 90, 2]
+    mats = [evdlib.to_cm(_sym(n, 300 + i), device=cuda) for i, n in enumerate(sizes)]
+    out, ms = serve.syevd_batched_native(mats, nstreams=3)
+    assert ms > 0
+    for A, (w, X) in zip(mats, out):
+        n = A.shape[0]
+        _, nb = serve.padded_shape(n)
+        w1, X1 = evdlib.syevd(A, 32, nb)
+        torch.cuda.synchronize()
+        assert torch.equal(w, w1) and torch.equal(X, X1)
+        _check(A.cpu(), w, X)
+
+
 def test_server_mix_matches_alone(cuda, evdlib):
     reqs = serve.poisson_stream(16, 400.0, 64, 600, seed=11)
     srv = serve.Server(nworkers=4, budget_bytes=8 * 10**9, device=cuda)
