@@ -1,5 +1,6 @@
 // myEVD <n> <b> <nb> [--dist uniform|gauss] [--seed S] [--reps R] [--no-check]
 //       [--input A.bin] [--save-input A.bin] [--output eig.bin]
+//       [--values] [--refine K]
 //
 // Command-line driver with the reference's surface (src/EVD/myEVD.cu:251-266:
 // three positional arguments; a wrong count prints the usage and returns 0).
@@ -10,6 +11,9 @@
 // the orthogonality / residual of the result.  --input reads A (n x n) from
 // record 0 of a binary matrix file instead; --save-input writes the generated
 // A; --output writes the eigenpairs (w, X) as a binary eigenpair file.
+// --values times the eigenvalues-only solve instead; --refine K runs K
+// Ogita-Aishima refinement iterations on the computed eigenpairs and prints
+// their time and the metrics after them.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -66,6 +70,7 @@ int main(int argc, char** argv) {
   int gauss = 0, reps = 1, check = 1;
   uint64_t seed = 3000;
   const char *in_path = nullptr, *save_path = nullptr, *out_path = nullptr;
+  int values_only = 0, refine = 0;
   for (int i = 4; i < argc; ++i) {
     if (!strcmp(argv[i], "--dist") && i + 1 < argc) gauss = !strcmp(argv[++i], "gauss");
     else if (!strcmp(argv[i], "--seed") && i + 1 < argc) seed = strtoull(argv[++i], 0, 10);
@@ -74,6 +79,8 @@ int main(int argc, char** argv) {
     else if (!strcmp(argv[i], "--input") && i + 1 < argc) in_path = argv[++i];
     else if (!strcmp(argv[i], "--save-input") && i + 1 < argc) save_path = argv[++i];
     else if (!strcmp(argv[i], "--output") && i + 1 < argc) out_path = argv[++i];
+    else if (!strcmp(argv[i], "--values")) values_only = 1;
+    else if (!strcmp(argv[i], "--refine") && i + 1 < argc) refine = atoi(argv[++i]);
   }
   printf("%s\nn=%ld, b=%ld, nb=%ld\n", evd_version(), n, b, nb);
   long wbytes = evd_syevd_work_size(n, b, nb);
@@ -110,6 +117,23 @@ int main(int argc, char** argv) {
     }
   }
   double t[6];
+  if (values_only) {
+    for (int r = 0; r < reps; ++r) {
+      int rc = evd_syevd_values(n, b, nb, A, n, w, work, wbytes, 1, 0);
+      if (rc != EVD_SUCCESS) {
+        printf("evd_syevd_values failed: %s\n", evd_status_string(rc));
+        return 2;
+      }
+      evd_syevd_last_timings(t);
+      printf("eigenvalues only %ldx%ld: sy2sb %.3f ms, chasing %.3f ms, multisection %.3f ms, "
+             "total %.3f ms\n", n, n, t[0], t[1], t[2], t[5]);
+    }
+    cudaFree(A);
+    cudaFree(X);
+    cudaFree(w);
+    cudaFree(work);
+    return 0;
+  }
   for (int r = 0; r < reps; ++r) {
     int rc = evd_syevd(n, b, nb, A, n, w, X, n, work, wbytes, 1, 0);
     if (rc != EVD_SUCCESS) {
@@ -127,6 +151,31 @@ int main(int argc, char** argv) {
     printf("SBR back %ldx%ld takes %.3f ms, tflops is %.3f\n", n, n, t[4], 2.0 * n3 / (t[4] * 1e9));
     printf("total EVD %ldx%ld takes %.3f ms, FP64-equivalent tflops is %.3f\n", n, n, t[5],
            16.0 / 3.0 * n3 / (t[5] * 1e9));
+  }
+  if (refine > 0) {
+    long rn = evd_refine_syev_work_size(n);
+    double* rw = nullptr;
+    if (rn <= 0) {
+      printf("refinement supports n <= 65535\n");
+      return 1;
+    }
+    CK(cudaMalloc(&rw, sizeof(double) * rn));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, 0));
+    int rc = evd_refine_syev(n, A, n, w, X, n, refine, rw, rn, 0);
+    CK(cudaEventRecord(e1, 0));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (rc != EVD_SUCCESS) {
+      printf("evd_refine_syev failed: %s\n", evd_status_string(rc));
+      return 2;
+    }
+    printf("refinement %d iteration(s) %ldx%ld takes %.3f ms (%.3f TFLOP/s FP64)\n", refine, n, n,
+           ms, 8.0 * refine * (double)n * n * n / (ms * 1e9));
+    cudaFree(rw);
   }
   if (out_path) {
     int rc = evd_write_eigenpairs_bin(out_path, n, w, X, n);

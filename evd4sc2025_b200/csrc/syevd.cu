@@ -15,6 +15,8 @@
 // makes a second call return early).
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "gemm_f64.cuh"
 
@@ -84,6 +86,15 @@ SyevdLayout layout(long n, long b, long nb) {
 
 thread_local double g_timings[6] = {0, 0, 0, 0, 0, 0};
 
+// NVTX range per stage (a profiler's timeline shows the stages by name; the
+// range closes on every return path)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 }  // namespace
 
 // err_out != nullptr: the chase's error word is not read here; its address is
@@ -111,32 +122,44 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
     for (auto& x : ev) EVD_CUDA_TRY(cudaEventCreate(&x));
     EVD_CUDA_TRY(cudaEventRecord(ev[0], st));
   }
-  // ---- stage 1: full -> band ----
-  EVD_TRY(copy_matrix(n, n, A, lda, OA, n, st));
-  EVD_TRY(copy_matrix(n, n, A, lda, dA, n, st));
-  EVD_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * n * n, st));
-  EVD_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * n * n, st));
-  EVD_TRY(sy2sb(n, n, b, nb, OA, n, dA, n, W, n, Y, n, Z, n, R, n, S,
-                (long)sy2sb_ws_doubles(n, b, nb), st));
+  {  // ---- stage 1: full -> band ----
+    NvtxRange r("evd_b200 sy2sb");
+    EVD_TRY(copy_matrix(n, n, A, lda, OA, n, st));
+    EVD_TRY(copy_matrix(n, n, A, lda, dA, n, st));
+    EVD_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * n * n, st));
+    EVD_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * n * n, st));
+    EVD_TRY(sy2sb(n, n, b, nb, OA, n, dA, n, W, n, Y, n, Z, n, R, n, S,
+                  (long)sy2sb_ws_doubles(n, b, nb), st));
+  }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[1], st));
-  // ---- stage 2: band -> tridiagonal ----
-  EVD_TRY(band_pack(n, b, dA, n, sub, 2 * b, st));
-  EVD_CUDA_TRY(cudaMemsetAsync(U, 0, sizeof(double) * n * n, st));
-  EVD_TRY(bulge_chase_async(n, b, sub, 2 * b, U, n, d, e, ich, st));
+  {  // ---- stage 2: band -> tridiagonal ----
+    NvtxRange r("evd_b200 bulge chasing");
+    EVD_TRY(band_pack(n, b, dA, n, sub, 2 * b, st));
+    EVD_CUDA_TRY(cudaMemsetAsync(U, 0, sizeof(double) * n * n, st));
+    EVD_TRY(bulge_chase_async(n, b, sub, 2 * b, U, n, d, e, ich, st));
+  }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[2], st));
-  // ---- tridiagonal D&C (eigenvectors straight into X) ----
-  EVD_TRY(stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
+  {  // ---- tridiagonal D&C (eigenvectors straight into X) ----
+    NvtxRange r("evd_b200 tridiagonal divide and conquer");
+    EVD_TRY(
+        stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
+  }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[3], st));
-  // ---- back transformations ----
-  // the T factors of the chasing reflectors go into OA (free after stage 1);
-  // for very small n they do not fit and the kernel rebuilds them itself
-  double* tbuf = ((size_t)q2_tbuf_doubles(n) <= (size_t)n * n) ? OA : nullptr;
-  EVD_TRY(q2_apply(false, n, n, U, n, X, ldX, tbuf, st));
+  {  // ---- back transformations ----
+    NvtxRange r("evd_b200 stage-2 back transformation");
+    // the T factors of the chasing reflectors go into OA (free after stage 1);
+    // for very small n they do not fit and the kernel rebuilds them itself
+    double* tbuf = ((size_t)q2_tbuf_doubles(n) <= (size_t)n * n) ? OA : nullptr;
+    EVD_TRY(q2_apply(false, n, n, U, n, X, ldX, tbuf, st));
+  }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[4], st));
-  const long npcols = ((n - 1) / b) * b;
-  EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, st));
-  EVD_TRY(sbr_apply_slabs(n, b, nb, W, n, Y, n, X, ldX, n, SB,
-                          (size_t)sbr_back_ws_doubles(n, b, nb), st));
+  {
+    NvtxRange r("evd_b200 stage-1 back transformation");
+    const long npcols = ((n - 1) / b) * b;
+    EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, st));
+    EVD_TRY(sbr_apply_slabs(n, b, nb, W, n, Y, n, X, ldX, n, SB,
+                            (size_t)sbr_back_ws_doubles(n, b, nb), st));
+  }
   EVD_CUDA_TRY(cudaMemcpyAsync(w, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   if (timed) {
     EVD_CUDA_TRY(cudaEventRecord(ev[5], st));

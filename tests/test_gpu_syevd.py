@@ -133,3 +133,19 @@ def test_syevd_any_order_zero_and_strided(cuda, evdlib):
     assert np.abs(w.cpu().numpy() - np.linalg.eigvalsh(A)).max() <= TOL_VAL * np.linalg.norm(A, 2)
     assert O.residual(A, w.cpu().numpy(), Xd.cpu().numpy()) <= TOL_RES
     assert float(Xbig[n:, :].abs().max()) == 0.0  # rows past n of X untouched
+
+
+@pytest.mark.parametrize("bad", [float("nan"), float("inf")])
+def test_non_finite_input_is_an_error(cuda, evdlib, bad):
+    """A non-finite entry makes the solve fail with a status (the tridiagonal
+    solver rejects non-finite input) instead of returning garbage; the
+    context stays usable for the next solve."""
+    n = 256
+    A = O.sym_gaussian(n, seed=12)
+    A[10, 3] = A[3, 10] = bad
+    Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
+    with pytest.raises(evdlib.EvdError) as e:
+        evdlib.syevd(Ad, 32, 64)
+    assert e.value.status < 0
+    w, X, res, orth = _run(cuda, evdlib, O.sym_gaussian(n, seed=13), 64)
+    assert res <= TOL_RES and orth <= TOL_ORT
