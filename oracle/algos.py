@@ -401,7 +401,7 @@ def haar_orthogonal(n: int, seed: int) -> np.ndarray:
 
 
 def spectrum(kind: str, n: int, seed: int) -> np.ndarray:
-    """Known spectra of the north-star inputs (sorted ascending).
+    """Known spectra of the benchmark inputs (sorted ascending).
 
     geometric: |lambda| from 1 down to 1e-6 (or `geometric1e10`: to 1e-10), random signs;
     uniform: uniform on [-1, 1]; clustered: 100 clusters of width 1e-10.

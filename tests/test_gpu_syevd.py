@@ -7,7 +7,7 @@ from oracle import algos as O
 
 pytestmark = pytest.mark.gpu
 
-# eigenvalues to 1e-12 relative to ||A||, residual and
+# accuracy bars: eigenvalues to 1e-12 relative to ||A||, residual and
 # orthogonality below 1e-13 (normalised by n, as the reference's checkMetric)
 TOL_VAL = 1e-12
 TOL_RES = 1e-13
