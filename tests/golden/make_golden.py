@@ -1,6 +1,6 @@
 """Generate golden fixtures from the reference's own GPU build.
 
-Runs on a GPU box (needs oracle/_ref/ref_driver, built by `make -C oracle`
+Runs on a machine with a B200 (needs oracle/_ref/ref_driver, built by `make -C oracle`
 from the reference sources).  For each (n, seed) it writes the seeded
 symmetrised Gaussian A = (G + G^T)/2 (numpy default_rng(seed)) to a raw
 column-major file, runs the reference pipeline on it (my_ZY_ZY_SBR_Vector ->
