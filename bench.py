@@ -203,6 +203,9 @@ def run_ours(args) -> int:
     fp64_peak = max(evd.fp64_peak_tflops() for _ in range(3))
     with torch.cuda.stream(stream):
         A, lam_known = _make_input(args.input, n, dev, 1234 + rank)
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()  # the generator's temporaries (QR of an n x n Gaussian)
+    with torch.cuda.stream(stream):
         ws = evd.Workspace(n, b, nb, device=dev)
         w = torch.empty(n, dtype=torch.float64, device=dev)
         X = evd.empty_cm(n, n, device=dev)
