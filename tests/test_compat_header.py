@@ -43,3 +43,46 @@ def test_compat_shims_compile(tmp_path):
     r = subprocess.run([nvcc, "-std=c++17", "-c", "-I", str(ROOT / "include"), str(src), "-o",
                         str(tmp_path / "use.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+C_USAGE = r'''
+#include <stdio.h>
+#include <cuda_runtime.h>
+#include "evd_b200.h"
+
+int use_c_api(long n, double* dA, double* dw, double* dX, long count, const long* orders,
+              double** A_ptrs, const long* ldas, double** w_ptrs, double** X_ptrs,
+              const long* ldXs, cudaStream_t stream) {
+  long nb = 256, wbytes = evd_syevd_work_size(n, 32, nb);
+  void* work = 0;
+  cudaMalloc(&work, wbytes);
+  int rc = evd_syevd(n, 32, nb, dA, n, dw, dX, n, work, wbytes, 0, stream);
+  if (rc != EVD_SUCCESS) fprintf(stderr, "%s\n", evd_status_string(rc));
+  long rn = evd_refine_syev_work_size(n);
+  double* rw = 0;
+  cudaMalloc((void**)&rw, rn * sizeof(double));
+  rc = evd_refine_syev(n, dA, n, dw, dX, n, 2, rw, rn, stream);
+  long bw = evd_syevd_batched_work_size(count, orders, 8);
+  void* bwork = 0;
+  cudaMalloc(&bwork, bw);
+  rc = evd_syevd_batched(count, orders, (const double* const*)A_ptrs, ldas, w_ptrs, X_ptrs,
+                         ldXs, 8, bwork, bw, stream);
+  evd_write_eigenpairs_bin("eig.bin", n, dw, dX, n);
+  evd_read_eigenpairs_bin("eig.bin", n, dw, dX, n);
+  return rc;
+}
+'''
+
+
+def test_c_header_compiles_as_c(tmp_path):
+    """include/evd_b200.h is plain C: the usage shown in the integration notes
+    compiles with the host C compiler."""
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no host C compiler")
+    src = tmp_path / "use.c"
+    src.write_text(C_USAGE)
+    r = subprocess.run([gcc, "-std=c11", "-Wall", "-Werror", "-c", "-I", str(ROOT / "include"),
+                        "-I", "/usr/local/cuda/include", str(src), "-o", str(tmp_path / "use.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
