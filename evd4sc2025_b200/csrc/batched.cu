@@ -56,10 +56,10 @@ extern "C" long evd_syevd_batched_work_size(long count, const long* n, int nstre
   return (long)(evd::slice_bytes(count, n) * workers + 256);
 }
 
-extern "C" int evd_syevd_batched(long count, const long* n, const double* const* A,
-                                 const long* lda, double* const* w, double* const* X,
-                                 const long* ldX, int nstreams, void* work, long lwork_bytes,
-                                 cudaStream_t stream) {
+static int syevd_batched_impl(long count, const long* n, const double* const* A,
+                              const long* lda, double* const* w, double* const* X,
+                              const long* ldX, int nstreams, void* work, long lwork_bytes,
+                              cudaStream_t stream) {
   if (count < 0 || nstreams < 1 || nstreams > 64) return EVD_ERR_INVALID_ARG;
   if (count == 0) return EVD_SUCCESS;
   if (!n || !A || !lda || !w || !X || !ldX || !work) return EVD_ERR_INVALID_ARG;
@@ -112,8 +112,13 @@ extern "C" int evd_syevd_batched(long count, const long* n, const double* const*
       cudaEventRecord(ends[t], streams[t]);
     };
     std::vector<std::thread> threads;
-    threads.reserve(workers);
-    for (int t = 0; t < workers; ++t) threads.emplace_back(worker, t);
+    try {
+      threads.reserve(workers);
+      for (int t = 0; t < workers; ++t) threads.emplace_back(worker, t);
+    } catch (...) {  // a thread could not start: the started ones stop and are joined
+      int expect = EVD_SUCCESS;
+      first_error.compare_exchange_strong(expect, EVD_ERR_HOST);
+    }
     for (auto& th : threads) th.join();
     rc = first_error.load();
     for (int t = 0; t < workers; ++t)
@@ -127,4 +132,17 @@ extern "C" int evd_syevd_batched(long count, const long* n, const double* const*
   }
   cudaEventDestroy(start);
   return rc;
+}
+
+// The C ABI never lets a C++ exception (host allocation, thread creation)
+// escape: it becomes EVD_ERR_HOST.
+extern "C" int evd_syevd_batched(long count, const long* n, const double* const* A,
+                                 const long* lda, double* const* w, double* const* X,
+                                 const long* ldX, int nstreams, void* work, long lwork_bytes,
+                                 cudaStream_t stream) {
+  try {
+    return syevd_batched_impl(count, n, A, lda, w, X, ldX, nstreams, work, lwork_bytes, stream);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
 }

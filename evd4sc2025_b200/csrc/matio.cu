@@ -135,7 +135,7 @@ int read_record(FILE* f, const RecHeader& h, double* A, long ldA) {
 using evd::File;
 using evd::RecHeader;
 
-extern "C" int evd_write_matrix_bin(const char* path, int append, long rows, long cols,
+static int evd_write_matrix_bin_impl(const char* path, int append, long rows, long cols,
                                     const double* A, long ldA) {
   if (!path || rows < 0 || cols < 0 || (rows * cols > 0 && (!A || ldA < rows)))
     return EVD_ERR_INVALID_ARG;
@@ -144,7 +144,7 @@ extern "C" int evd_write_matrix_bin(const char* path, int append, long rows, lon
   return evd::write_record(F.f, rows, cols, A, ldA);
 }
 
-extern "C" long evd_matrix_bin_count(const char* path) {
+static long evd_matrix_bin_count_impl(const char* path) {
   if (!path) return EVD_ERR_INVALID_ARG;
   File F(path, "rb");
   if (!F.f) return EVD_ERR_IO;
@@ -159,7 +159,7 @@ extern "C" long evd_matrix_bin_count(const char* path) {
   }
 }
 
-extern "C" int evd_matrix_bin_shape(const char* path, long index, long* rows, long* cols) {
+static int evd_matrix_bin_shape_impl(const char* path, long index, long* rows, long* cols) {
   if (!path || !rows || !cols) return EVD_ERR_INVALID_ARG;
   File F(path, "rb");
   if (!F.f) return EVD_ERR_IO;
@@ -170,7 +170,7 @@ extern "C" int evd_matrix_bin_shape(const char* path, long index, long* rows, lo
   return EVD_SUCCESS;
 }
 
-extern "C" int evd_read_matrix_bin(const char* path, long index, long rows, long cols, double* A,
+static int evd_read_matrix_bin_impl(const char* path, long index, long rows, long cols, double* A,
                                    long ldA) {
   if (!path || rows < 0 || cols < 0 || (rows * cols > 0 && (!A || ldA < rows)))
     return EVD_ERR_INVALID_ARG;
@@ -182,7 +182,7 @@ extern "C" int evd_read_matrix_bin(const char* path, long index, long rows, long
   return evd::read_record(F.f, h, A, ldA);
 }
 
-extern "C" int evd_write_eigenpairs_bin(const char* path, long n, const double* w,
+static int evd_write_eigenpairs_bin_impl(const char* path, long n, const double* w,
                                         const double* X, long ldX) {
   if (!path || n < 0 || (n > 0 && (!w || !X || ldX < n))) return EVD_ERR_INVALID_ARG;
   File F(path, "wb");
@@ -191,7 +191,7 @@ extern "C" int evd_write_eigenpairs_bin(const char* path, long n, const double* 
   return evd::write_record(F.f, n, n, X, ldX);
 }
 
-extern "C" int evd_read_eigenpairs_bin(const char* path, long n, double* w, double* X, long ldX) {
+static int evd_read_eigenpairs_bin_impl(const char* path, long n, double* w, double* X, long ldX) {
   if (!path || n < 0 || (n > 0 && (!w || !X || ldX < n))) return EVD_ERR_INVALID_ARG;
   File F(path, "rb");
   if (!F.f) return EVD_ERR_IO;
@@ -206,7 +206,7 @@ extern "C" int evd_read_eigenpairs_bin(const char* path, long n, double* w, doub
 
 // ---- CSV in the reference's layout (one matrix row per line, commas) ----
 
-extern "C" int evd_write_matrix_csv(const char* path, long rows, long cols, const double* A,
+static int evd_write_matrix_csv_impl(const char* path, long rows, long cols, const double* A,
                                     long ldA) {
   if (!path || rows < 0 || cols < 0 || (rows * cols > 0 && (!A || ldA < rows)))
     return EVD_ERR_INVALID_ARG;
@@ -227,7 +227,7 @@ extern "C" int evd_write_matrix_csv(const char* path, long rows, long cols, cons
 
 // Shape query (A == NULL) or read.  Every line must have the same number of
 // comma-separated values.
-extern "C" int evd_read_matrix_csv(const char* path, long* rows, long* cols, double* A, long ldA) {
+static int evd_read_matrix_csv_impl(const char* path, long* rows, long* cols, double* A, long ldA) {
   if (!path || !rows || !cols) return EVD_ERR_INVALID_ARG;
   File F(path, "r");
   if (!F.f) return EVD_ERR_IO;
@@ -273,3 +273,74 @@ extern "C" int evd_read_matrix_csv(const char* path, long* rows, long* cols, dou
                             sizeof(double) * r, c));
   return EVD_SUCCESS;
 }
+
+// C ABI wrappers: a C++ exception (host memory for the staging buffers)
+// becomes EVD_ERR_HOST.
+extern "C" int evd_write_matrix_bin(const char* path, int append, long rows, long cols,
+                                    const double* A, long ldA) {
+  try {
+    return evd_write_matrix_bin_impl(path, append, rows, cols, A, ldA);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" long evd_matrix_bin_count(const char* path) {
+  try {
+    return evd_matrix_bin_count_impl(path);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_matrix_bin_shape(const char* path, long index, long* rows, long* cols) {
+  try {
+    return evd_matrix_bin_shape_impl(path, index, rows, cols);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_read_matrix_bin(const char* path, long index, long rows, long cols, double* A,
+                                   long ldA) {
+  try {
+    return evd_read_matrix_bin_impl(path, index, rows, cols, A, ldA);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_write_eigenpairs_bin(const char* path, long n, const double* w,
+                                        const double* X, long ldX) {
+  try {
+    return evd_write_eigenpairs_bin_impl(path, n, w, X, ldX);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_read_eigenpairs_bin(const char* path, long n, double* w, double* X, long ldX) {
+  try {
+    return evd_read_eigenpairs_bin_impl(path, n, w, X, ldX);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_write_matrix_csv(const char* path, long rows, long cols, const double* A,
+                                    long ldA) {
+  try {
+    return evd_write_matrix_csv_impl(path, rows, cols, A, ldA);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_read_matrix_csv(const char* path, long* rows, long* cols, double* A, long ldA) {
+  try {
+    return evd_read_matrix_csv_impl(path, rows, cols, A, ldA);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+

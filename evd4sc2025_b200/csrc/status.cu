@@ -10,6 +10,7 @@ extern "C" const char* evd_status_string(int status) {
     case EVD_ERR_NO_CONVERGENCE: return "iteration did not converge";
     case EVD_ERR_WORKSPACE: return "workspace too small";
     case EVD_ERR_IO: return "file I/O error";
+    case EVD_ERR_HOST: return "host resource failure (threads or host memory)";
     default: return "unknown status";
   }
 }

@@ -238,8 +238,9 @@ class Result:
     arrival: float
     admitted: float
     done: float
-    w: torch.Tensor
-    X: torch.Tensor
+    w: torch.Tensor | None
+    X: torch.Tensor | None
+    error: str | None = None           # set when the solve failed (w, X are None)
 
     @property
     def latency(self) -> float:
@@ -295,12 +296,17 @@ class Server:
                 if not self._ready:
                     return
                 _, _, req, t_adm = heapq.heappop(self._ready)
-            w, X = self.solve_fn(k, req.A)
+            err = None
+            try:
+                w, X = self.solve_fn(k, req.A)
+            except Exception as e:  # a failed request must still return its memory
+                w = X = None
+                err = f"{type(e).__name__}: {e}"
             t_done = time.perf_counter() - t0
             with self._cv:
                 self._in_use -= req.bytes
                 self._results.append(Result(req.rid, req.A.shape[0], req.arrival, t_adm, t_done,
-                                            w, X))
+                                            w, X, err))
                 self._cv.notify_all()
 
     def run(self, requests: list[Request]) -> dict:
@@ -349,6 +355,7 @@ class Server:
                 return float("nan")
             return lat[min(len(lat) - 1, int(math.ceil(p / 100.0 * len(lat))) - 1)]
         return {"requests": len(self._results), "wall_s": wall,
+                "failed": sum(1 for r in self._results if r.error is not None),
                 "solves_per_s": len(self._results) / wall if wall > 0 else float("nan"),
                 "p50_s": pct(50), "p99_s": pct(99), "max_in_flight_bytes": self.max_in_flight_bytes}
 

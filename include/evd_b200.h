@@ -37,6 +37,7 @@ extern "C" {
 #define EVD_ERR_NO_CONVERGENCE (-4)/* an iterative solver did not converge        */
 #define EVD_ERR_WORKSPACE (-5)     /* workspace smaller than the size query says  */
 #define EVD_ERR_IO (-6)            /* a file could not be opened, read or written */
+#define EVD_ERR_HOST (-7)          /* a host resource failed (threads, host memory) */
 
 /* Human-readable text for a status code (static storage). */
 const char* evd_status_string(int status);

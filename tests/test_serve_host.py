@@ -135,3 +135,17 @@ def test_server_runs_twice():
     assert first["requests"] == 3
     second = srv.run(_fake_requests([6, 7], gap=0.0))
     assert second["requests"] == 2 and len(srv.results) == 2
+
+
+def test_failed_solve_returns_its_memory():
+    """A request whose solve raises is reported as failed and gives its memory
+    back, so the requests behind it are still admitted and served."""
+    def solve(k, A):
+        if A.shape[0] == 5:
+            raise RuntimeError("bad input")
+        return A, A
+    srv = serve.Server(nworkers=1, budget_bytes=6, solve_fn=solve, footprint_fn=lambda n: n)
+    stats = srv.run(_fake_requests([5, 6, 4, 6], gap=0.0))
+    assert stats["requests"] == 4 and stats["failed"] == 1
+    bad = [r for r in srv.results if r.error is not None]
+    assert len(bad) == 1 and bad[0].n == 5 and "bad input" in bad[0].error
