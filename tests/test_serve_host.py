@@ -149,3 +149,23 @@ def test_failed_solve_returns_its_memory():
     assert stats["requests"] == 4 and stats["failed"] == 1
     bad = [r for r in srv.results if r.error is not None]
     assert len(bad) == 1 and bad[0].n == 5 and "bad input" in bad[0].error
+
+
+def test_shipped_tuning_table_is_consistent():
+    """The measured B200 table: every entry times every candidate nb that fits
+    its order, its best nb is the fastest one, and every order 1..65536 gets a
+    valid (n', nb) from solve_shape."""
+    import math
+
+    from evd4sc2025_b200 import autotune
+    table = autotune.load(autotune.DEFAULT_TABLE)
+    assert table and table["b"] == 32 and len(table["entries"]) >= 10
+    for e in table["entries"]:
+        ms = {int(k): v for k, v in e["ms"].items()}
+        assert set(ms) == set(autotune._candidates(e["n"]))
+        assert all(v > 0 and math.isfinite(v) for v in ms.values())
+        assert e["nb"] == min(ms, key=ms.get)
+    for n in list(range(1, 300)) + [1000, 1023, 1025, 4095, 5152, 8191, 16384, 40000, 65536]:
+        np_, nb = serve.solve_shape(n)
+        assert np_ >= max(n, 64) and np_ % nb == 0 and 32 <= nb <= 1024
+        assert (nb // 32) & (nb // 32 - 1) == 0
