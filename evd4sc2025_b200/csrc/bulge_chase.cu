@@ -25,7 +25,7 @@
 //    overlaps that work; the previous tile is stored right after the B1 update.
 //  * S2 <- H S2 H uses the symmetric rank-2 form (y = S u, v = y - (u^T y/2) u,
 //    S -= u v^T + v u^T) and every block update runs on 128 threads (4 per
-//    row/column, two shuffle steps per dot product).
+//    row/column; each dot product ends with a 4-lane sum on the DMMA pipe).
 //  * every wait is bounded in time; on timeout the kernel records an error
 //    word, all CTAs drain, and the host returns EVD_ERR_TIMEOUT.
 #include <mutex>
