@@ -20,6 +20,14 @@ bulge chasing kernel  -> :func:`bulge_chase`
 ``computerQFromWY``   -> :func:`q_from_wy`
 ``checkOrthogonality`` -> :func:`check_orthogonality`
 host ``LAPACKE_dstedc`` -> :func:`stedc` (device divide and conquer)
+``panelQR<float/half>``, ``tc_ozimmu_syr2k<float/half>``, ``tc_syr2k``
+                      -> :mod:`evd4sc2025_b200.lowprec`
+``writeMatrixToCsvV2`` / ``readMatrixFromFile`` -> :mod:`evd4sc2025_b200.matio`
+
+Beyond the reference: :func:`syevd_values` (eigenvalues only), any order n in
+:func:`syevd`, :func:`refine_syev` (Ogita-Aishima refinement),
+:mod:`evd4sc2025_b200.serve` (batched solves, serving loop),
+:mod:`evd4sc2025_b200.autotune` (nb per order).
 """
 from __future__ import annotations
 
