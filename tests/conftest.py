@@ -4,7 +4,6 @@
 fixtures, host logic, C-ABI exports).  `pytest -m gpu` runs on a B200 and
 checks the CUDA path, called through the C ABI, against the oracle.
 """
-import os
 import pathlib
 import sys
 

@@ -9,7 +9,6 @@ own slot, and (3) equal the 128-byte swizzle the MMA descriptor declares
 address r * 128 + c * 16).  The global side must read each (row, chunk) of
 the packed operand exactly once per stage.
 """
-import numpy as np
 
 TILE_ROWS, CHUNKS, THREADS = 128, 8, 128
 
