@@ -41,7 +41,7 @@ __all__ = [
     "EvdError", "lib", "empty_cm", "to_cm", "dgemm", "syr2k", "band_pack", "bulge_chase",
     "tsqr", "panel_qr", "sy2sb", "stedc", "bc_back", "bc_back_apply", "wy_from_slide",
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
-    "syevd_values", "eigvalsh", "stebz", "refine_syev",
+    "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -400,16 +400,25 @@ def syevd_values(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | N
 eigvalsh = syevd_values
 
 
-def refine_syev(A: torch.Tensor, X: torch.Tensor, iters: int = 2, w: torch.Tensor | None = None,
-                stream=None):
-    """Ogita-Aishima refinement of approximate eigenvectors X (in place) of
-    the symmetric FP64 matrix A; returns (w, X) with w the refined
-    eigenvalues in the column order of X."""
-    n = A.shape[0]
+def refine_work(n: int, device="cuda") -> torch.Tensor:
+    """Workspace of :func:`refine_syev` for order n (allocate it once and pass
+    it to every call to keep allocation out of a timed loop)."""
     nw = int(lib().evd_refine_syev_work_size(n))
     if nw <= 0:
         raise EvdError("evd_refine_syev_work_size", -1)
-    work = torch.empty(nw, dtype=F64, device=A.device)
+    return torch.empty(nw, dtype=F64, device=device)
+
+
+def refine_syev(A: torch.Tensor, X: torch.Tensor, iters: int = 2, w: torch.Tensor | None = None,
+                stream=None, work: torch.Tensor | None = None):
+    """Ogita-Aishima refinement of approximate eigenvectors X (in place) of
+    the symmetric FP64 matrix A; returns (w, X) with w the refined
+    eigenvalues in the column order of X.  ``work`` (from
+    :func:`refine_work`) is allocated per call when omitted."""
+    n = A.shape[0]
+    if work is None:
+        work = refine_work(n, A.device)
+    nw = work.numel()
     if w is None:
         w = torch.empty(n, dtype=F64, device=A.device)
     pa, lda = _cm(A, "A")

@@ -469,12 +469,7 @@ __global__ void __launch_bounds__(kQThreads, 2)
 template <bool FWD, bool PRE>
 int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
               long ldX, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    EVD_CUDA_TRY(cudaFuncSetAttribute(q2_mma_kernel<FWD, PRE>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
-    attr = true;
-  }
+  EVD_TRY(smem_attr_once((const void*)q2_mma_kernel<FWD, PRE>, (int)kQSmem));
   int grid = ceil_div_i((int)ncols, kQW * kQCols);
   q2_mma_kernel<FWD, PRE><<<grid, kQThreads, kQSmem, st>>>((int)n, (int)ncols, U, ldU, Tg, X,
                                                            ldX);

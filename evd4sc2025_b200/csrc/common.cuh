@@ -78,8 +78,14 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 
 inline int ceil_div_i(long a, long b) { return (int)((a + b - 1) / b); }
 
+// SM count of the current device (cached per device; thread-safe).
 int device_sm_count();
 void note_launch();
+
+// Raises `func`'s dynamic shared-memory limit to `bytes` once per (device,
+// kernel); thread-safe, so host threads driving several devices or streams
+// (the batched solver) may launch the same kernel concurrently.
+int smem_attr_once(const void* func, int bytes);
 
 // Reads a device error word written by a kernel (synchronises `st`) and maps
 // it to an EVD_* status.

@@ -620,12 +620,7 @@ int launch_cfg(GemmArgs p, int grid_x, int grid_y, cudaStream_t st) {
       STAGES * (ATile<TA, BM, BK>::kSize + BTile<TB, BN, BK>::kSize) * sizeof(double);
   auto kern = FAST ? dgemm_fast_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>
                    : dgemm_kernel<TA, TB, BM, BN, BK, WM, WN, STAGES, MMA>;
-  static bool attr_set = false;  // per instantiation; set once per process
-  if (!attr_set) {
-    EVD_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    attr_set = true;
-  }
+  EVD_TRY(smem_attr_once((const void*)kern, (int)smem));
   kern<<<dim3(grid_x, grid_y), NT, smem, st>>>(p);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
@@ -669,17 +664,6 @@ int dispatch_shape(GemmArgs p, long batch, cudaStream_t st) {
 }
 
 }  // namespace
-
-int device_sm_count() {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
-  return sms;
-}
 
 static bool aligned16_all(const double* ptr, long ld, long stride) {
   return aligned16(ptr, ld) && ((stride & 1) == 0);

@@ -7,6 +7,8 @@
 //   orthogonality ||X^T X - I||_F / n.
 // Norms are reduced in a fixed order (per-block partials, then one block), so
 // the result is deterministic.
+#include <mutex>
+
 #include "common.cuh"
 #include "gemm_f64.cuh"
 
@@ -64,16 +66,18 @@ __device__ double g_metric_partials[kRedBlocks + 16];
 
 }  // namespace
 
+// Device address of g_metric_partials on the current device (the runtime keeps
+// one copy of the module per device), cached per device under a lock.
 static int metric_scratch(double** p) {
-  static double* dev = nullptr;  // per process; the runtime keeps one module per device
+  constexpr int kMaxDev = 64;
+  static std::mutex mu;
+  static double* addr[kMaxDev] = {};
   int d = -1;
-  static int dev_id = -2;
   EVD_CUDA_TRY(cudaGetDevice(&d));
-  if (dev == nullptr || d != dev_id) {
-    EVD_CUDA_TRY(cudaGetSymbolAddress((void**)&dev, g_metric_partials));
-    dev_id = d;
-  }
-  *p = dev;
+  if (d < 0 || d >= kMaxDev) return EVD_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(mu);
+  if (addr[d] == nullptr) EVD_CUDA_TRY(cudaGetSymbolAddress((void**)&addr[d], g_metric_partials));
+  *p = addr[d];
   return EVD_SUCCESS;
 }
 

@@ -521,17 +521,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 constexpr size_t kFinishDyn = 2 * kSub * 33 * sizeof(double);
 
 int finish_attr() {
-  static bool done = false;
-  if (!done) {
-    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_finish_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kFinishDyn));
-    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_up_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kTileSmem));
-    EVD_CUDA_TRY(cudaFuncSetAttribute(tsqr_q_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kTileSmem));
-    done = true;
-  }
+  EVD_TRY(smem_attr_once((const void*)tsqr_finish_kernel, (int)kFinishDyn));
+  EVD_TRY(smem_attr_once((const void*)tsqr_up_kernel, (int)kTileSmem));
+  EVD_TRY(smem_attr_once((const void*)tsqr_q_kernel, (int)kTileSmem));
   return EVD_SUCCESS;
 }
 

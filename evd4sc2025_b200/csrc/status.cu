@@ -19,10 +19,39 @@ extern "C" const char* evd_version(void) { return "evd_b200 0.1 sm_100a"; }
 
 // ---- launch accounting and the FP64 peak probe ----------------------------
 #include <atomic>
+#include <mutex>
+#include <set>
+#include <utility>
 
 namespace evd {
 static std::atomic<long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+int device_sm_count() {
+  constexpr int kMaxDev = 64;
+  static std::atomic<int> sms[kMaxDev] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 148;
+  int v = sms[dev].load(std::memory_order_relaxed);
+  if (v <= 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    sms[dev].store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+
+int smem_attr_once(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  EVD_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({dev, func})) return EVD_SUCCESS;
+  EVD_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert({dev, func});
+  return EVD_SUCCESS;
+}
 
 namespace {
 // Each warp keeps 8 independent 8x8x4 DMMA accumulators busy; 2 CTAs per SM.

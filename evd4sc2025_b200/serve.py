@@ -116,11 +116,22 @@ class StreamSolver:
         n = A.shape[0]
         if nb is None:
             _, nb = solve_shape(n)
+        # The results belong to the caller's stream; the solve runs on this
+        # worker's stream, which first waits for the caller's pending work
+        # (A may still be being produced there).  record_stream keeps the
+        # caching allocator from handing A, w or X to other work before this
+        # stream is done with them.
+        caller = torch.cuda.current_stream(self.device)
+        w = torch.empty(n, dtype=F64, device=self.device)
+        X = empty_cm(n, n, device=self.device)
+        self.stream.wait_stream(caller)
+        w.record_stream(self.stream)
+        X.record_stream(self.stream)
+        if A.is_cuda:
+            A.record_stream(self.stream)
         with torch.cuda.stream(self.stream):
             Ab = self._ensure(n, nb)
             Ab.copy_(A, non_blocking=True)
-            w = torch.empty(n, dtype=F64, device=self.device)
-            X = empty_cm(n, n, device=self.device)
             pa, lda = _cm(Ab, "A")
             px, ldx = _cm(X, "X")
             call("evd_syevd", n, 32, nb, pa, lda, _ptr(w), px, ldx, _ptr(self._ws),

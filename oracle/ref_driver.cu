@@ -11,7 +11,10 @@
 // main reads uninitialised com[] and padding rows), and stage times are
 // printed as one JSON line.  Optional outputs: eigenvalues and eigenvectors.
 //
-// usage: ref_driver n b nb input(.bin|-) out_prefix(|-) [reps]
+// usage: ref_driver n b nb input(.bin|-) out_prefix(|-) [reps] [outputs]
+//   outputs "all" (default): w, X, d, e files; "w": eigenvalues only, plus the
+//   result's residual ||AX - X diag(w)||_F / ||A||_F and orthogonality
+//   ||X^T X - I||_F (cuBLAS, after the timed solves) as one JSON line.
 #include <cooperative_groups.h>
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
@@ -71,6 +74,7 @@ int main(int argc, char** argv) {
   long n = atol(argv[1]), b = atol(argv[2]), nb = atol(argv[3]);
   std::string in = argv[4], outp = argv[5];
   int reps = argc > 6 ? atoi(argv[6]) : 1;
+  const std::string outputs = argc > 7 ? argv[7] : "all";
   long m = n;
   cusolverDnHandle_t cusolver_handle;
   cublasHandle_t cublas_handle;
@@ -198,7 +202,31 @@ int main(int argc, char** argv) {
            total_ms);
     fflush(stdout);
   }
-  if (outp != "-") {
+  if (outp != "-" && outputs == "w") {
+    FILE* f = fopen((outp + "_w.bin").c_str(), "wb");
+    fwrite(hS.data(), sizeof(double), n, f);
+    fclose(f);
+    // accuracy of the last result (dT = A, dY = X, hS = w): R = A X - X diag(w)
+    double one = 1.0, zz = 0.0, mone = -1.0, ra = 0.0, rr = 0.0, ro = 0.0;
+    CK(cudaMemcpy(dU, hS.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    cublasDgemm(cublas_handle, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &one, dT, m, dY, m, &zz, dwork, n);
+    cublasDdgmm(cublas_handle, CUBLAS_SIDE_RIGHT, n, n, dY, m, dU, 1, dQ, n);
+    cublasDgeam(cublas_handle, CUBLAS_OP_N, CUBLAS_OP_N, n, n, &one, dwork, n, &mone, dQ, n, dwork, n);
+    cublasDnrm2(cublas_handle, n * n, dwork, 1, &rr);
+    cublasDnrm2(cublas_handle, m * n, dT, 1, &ra);
+    // X^T X - I
+    cublasDgemm(cublas_handle, CUBLAS_OP_T, CUBLAS_OP_N, n, n, n, &one, dY, m, dY, m, &zz, dwork, n);
+    {
+      dim3 gs((n + 31) / 32), bs(32);
+      launchKernel_ClearMatrix(dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 32), n, n, dQ, n);
+      launchKernel_setMetrixTrValue(gs, bs, n, n, dQ, n, 1.0);
+    }
+    cublasDgeam(cublas_handle, CUBLAS_OP_N, CUBLAS_OP_N, n, n, &one, dwork, n, &mone, dQ, n, dwork, n);
+    cublasDnrm2(cublas_handle, n * n, dwork, 1, &ro);
+    CK(cudaDeviceSynchronize());
+    printf("{\"accuracy\": {\"resid_fro_rel\": %.6e, \"orth_fro\": %.6e, \"resid\": %.6e, "
+           "\"orth\": %.6e}}\n", rr / ra, ro, rr / ra / n, ro / n);
+  } else if (outp != "-") {
     std::vector<double> X((size_t)n * n);
     CK(cudaMemcpy2D(X.data(), sizeof(double) * n, dY, sizeof(double) * m, sizeof(double) * n, n,
                     cudaMemcpyDeviceToHost));

@@ -11,8 +11,9 @@ compressed:
   X8  the first 8 eigenvector columns of the reference's X = Q^T Z
   resid, orth  the reference result's residual / orthogonality (computed here)
 
-usage: python tests/golden/make_golden.py OUT_DIR
-Fixtures are small (n <= 2048); A itself is regenerated from the seed.
+usage: python tests/golden/make_golden.py OUT_DIR [n ...]   (default: every case)
+Fixtures are small (n <= 4096; vectors: 8 columns); A itself is regenerated
+from the seed.
 """
 from __future__ import annotations
 
@@ -28,14 +29,16 @@ sys.path.insert(0, str(ROOT))
 
 from oracle import algos as O  # noqa: E402
 
-CASES = [(1024, 11), (2048, 12)]
+CASES = [(1024, 11), (2048, 12), (4096, 13)]
 
 
-def main(out_dir: str) -> int:
+def main(out_dir: str, only: list[int] | None = None) -> int:
     out = pathlib.Path(out_dir)
     out.mkdir(parents=True, exist_ok=True)
     drv = ROOT / "oracle" / "_ref" / "ref_driver"
     for n, seed in CASES:
+        if only and n not in only:
+            continue
         A = O.sym_gaussian(n, seed)
         fin = out / f"A_{n}_{seed}.bin"
         np.asfortranarray(A).T.tofile(fin)  # column-major bytes
@@ -61,4 +64,5 @@ def main(out_dir: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else str(HERE)))
+    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else str(HERE),
+                  [int(a) for a in sys.argv[2:]] or None))
