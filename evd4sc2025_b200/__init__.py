@@ -41,7 +41,8 @@ __all__ = [
     "EvdError", "lib", "empty_cm", "to_cm", "dgemm", "syr2k", "band_pack", "bulge_chase",
     "tsqr", "panel_qr", "sy2sb", "stedc", "bc_back", "bc_back_apply", "wy_from_slide",
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
-    "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work",
+    "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work", "dgemm_ozaki",
+    "dgemm_ozaki_work_size", "ozaki_bits",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -108,6 +109,40 @@ def dgemm(transa: str, transb: str, alpha: float, A: torch.Tensor, B: torch.Tens
     call("evd_dgemm", transa.encode(), transb.encode(), m, n, k, alpha, pa, lda, pb, ldb,
          beta, pc, ldc, _stream(stream))
     return Cm
+
+
+def dgemm_ozaki(transa: str, transb: str, alpha: float, A: torch.Tensor, B: torch.Tensor,
+                beta: float, Cm: torch.Tensor, moduli: int = 14, work: torch.Tensor | None = None,
+                stream=None) -> torch.Tensor:
+    """C = alpha*op(A)*op(B) + beta*C (in place) as an emulated FP64 product on
+    the integer tensor cores (Ozaki scheme II with ``moduli`` moduli; 14 give
+    53-bit operands).  ``work``: a uint8 device tensor of at least
+    :func:`dgemm_ozaki_work_size` bytes (allocated per call when omitted)."""
+    m, n = Cm.shape
+    k = A.shape[0] if transa.lower() == "t" else A.shape[1]
+    need = dgemm_ozaki_work_size(transa, transb, m, n, k, moduli)
+    if work is None:
+        work = torch.empty(need, dtype=torch.uint8, device=Cm.device)
+    pa, lda = _cm(A, "A")
+    pb, ldb = _cm(B, "B")
+    pc, ldc = _cm(Cm, "C")
+    call("evd_dgemm_ozaki", transa.encode(), transb.encode(), m, n, k, alpha, pa, lda, pb, ldb,
+         beta, pc, ldc, moduli, _ptr(work), work.numel(), _stream(stream))
+    return Cm
+
+
+def dgemm_ozaki_work_size(transa: str, transb: str, m: int, n: int, k: int,
+                          moduli: int = 14) -> int:
+    """Workspace bytes of :func:`dgemm_ozaki`."""
+    need = int(lib().evd_dgemm_ozaki_work_size(transa.encode(), transb.encode(), m, n, k, moduli))
+    if need <= 0:
+        raise EvdError("evd_dgemm_ozaki_work_size", -1)
+    return need
+
+
+def ozaki_bits(moduli: int, k: int) -> int:
+    """Integer bits P of the emulated product's operands."""
+    return int(lib().evd_ozaki_bits(moduli, k))
 
 
 def syr2k(alpha: float, A: torch.Tensor, B: torch.Tensor, beta: float, Cm: torch.Tensor,

@@ -1,0 +1,708 @@
+// Emulated FP64 matrix products on the integer tensor cores (Ozaki scheme II:
+// Ozaki, Uchino, Imamura, "Ozaki Scheme II: A GEMM-oriented emulation of
+// floating-point matrix multiplication using an integer modular technique",
+// 2025).  The reference has no counterpart: its products are cuBLAS DGEMMs
+// (api/TCblas/tc_ozimmu_syr2k.cu:54-192 calls cublasDgemm), and this is the
+// contraction that the mixed-precision solve and the eigenpair refinement run
+// instead of FP64 DMMA.
+//
+// D = alpha * op(A) op(B) + beta * C + diag * I, with op(A) M x K, op(B) K x N:
+//   1. every row i of op(A) is scaled by 2^e_i and rounded to an integer
+//      vector a_i with ||a_i||_2 <= 2^P (likewise every column j of op(B) by
+//      2^f_j to b_j), so |a_i . b_j| <= 2^2P < Mod / 2;
+//   2. for each of N pairwise coprime moduli p_l <= 256 the residues
+//      a mod p_l, b mod p_l (symmetric range, int8) are multiplied EXACTLY by
+//      one tcgen05 kind::i8 GEMM with INT32 accumulation (|sum| <= K 2^14 <
+//      2^31 for K < 2^17), and the epilogue stores (a . b) mod p_l as a byte;
+//   3. the Chinese remainder theorem rebuilds a_i . b_j in (-Mod/2, Mod/2)
+//      exactly (128-bit integers), which is scaled back by 2^-(e_i + f_j).
+// The only rounding is step 1: |D_ij - (op(A) op(B))_ij| <= ~ sqrt(K) 2^-P
+// ||op(A)_i|| ||op(B)_j||.  14 moduli give P = 53 (FP64 inputs); fewer moduli
+// trade accuracy for speed (P ~ 4 N - 2).
+//
+// The int8 GEMM (one launch for all moduli, blockIdx.y = modulus): CTA tile
+// 256 x 256 as two M128 N256 K32 tcgen05.mma per K step into two 256-column
+// INT32 accumulators in tensor memory (all 512 columns); both operands K-major
+// (rows of 128 bytes), brought in by TMA (cp.async.bulk.tensor, 128-byte
+// swizzle, this GPU's own memory only, no multicast) through a 3-stage
+// mbarrier pipeline: one thread issues the copies, one thread issues the
+// MMAs, and all four warps run the epilogue (tcgen05.ld, Barrett reduction,
+// byte stores).  Every wait is bounded (2 s) and reports EVD_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <math.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "ozaki.cuh"
+
+namespace evd {
+namespace {
+
+// ------------------------------------------------------------------ moduli
+// 256 and odd pairwise coprime numbers below it, largest first (their prime
+// factors: 2; 3 5 17; 11 23; 251; 13 19; 241; 239; 233; 229; 227; 223; 7 31;
+// 211; 199; 197; 193; 191; 181; 179; 173).
+constexpr int kModTable[kOzMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+typedef unsigned __int128 u128;
+
+struct OzConsts {
+  int nmod;
+  int p[kOzMaxMod];
+  unsigned magic[kOzMaxMod];   // floor(2^32 / p): Barrett quotient estimate
+  double invp[kOzMaxMod];      // 1 / p
+  unsigned long long wlo[kOzMaxMod], whi[kOzMaxMod];  // CRT weights (M / p) ((M / p)^-1 mod p)
+  unsigned long long mlo, mhi;  // Mod = prod p
+  double invM;                  // 1 / Mod
+  int P;                        // bits of the integer operands (row norm <= 2^P)
+};
+
+__host__ __device__ __forceinline__ u128 mk128(unsigned long long lo, unsigned long long hi) { return ((u128)hi << 64) | lo; }
+
+// modular inverse of a mod p (p <= 256, gcd = 1), by search
+int inv_mod(u128 a, int p) {
+  const int r = (int)(a % (u128)p);
+  for (int x = 1; x < p; ++x)
+    if ((r * x) % p == 1) return x;
+  return 0;
+}
+
+OzConsts make_consts(int nmod, long K) {
+  OzConsts c{};
+  c.nmod = nmod;
+  u128 M = 1;
+  for (int l = 0; l < nmod; ++l) M *= (u128)kModTable[l];
+  for (int l = 0; l < nmod; ++l) {
+    const int p = kModTable[l];
+    c.p[l] = p;
+    c.magic[l] = (unsigned)(((unsigned long long)1 << 32) / (unsigned long long)p);
+    c.invp[l] = 1.0 / (double)p;
+    const u128 Mi = M / (u128)p;
+    const u128 w = Mi * (u128)inv_mod(Mi, p);  // < M: (M/p) * (p - 1) < M
+    c.wlo[l] = (unsigned long long)w;
+    c.whi[l] = (unsigned long long)(w >> 64);
+  }
+  c.mlo = (unsigned long long)M;
+  c.mhi = (unsigned long long)(M >> 64);
+  const long double Md = (long double)c.mhi * 18446744073709551616.0L + (long double)c.mlo;
+  c.invM = (double)(1.0L / Md);
+  // largest P with (2^P + sqrt(K)/2)^2 < M/2 (the rounding of each element
+  // adds at most 1/2, so a row's norm grows by at most sqrt(K)/2)
+  const long double lim = sqrtl(Md / 2.0L) * (1.0L - 1e-12L) - sqrtl((long double)K) / 2.0L;
+  int P = (int)floorl(log2l(lim));
+  c.P = std::min(P, 53);
+  return c;
+}
+
+// -------------------------------------------------------------- utilities
+constexpr unsigned long long kOzWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for phase `parity`; false (error recorded) after kOzWaitNs
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 0;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63u) == 63u && gtimer() - t0 > kOzWaitNs) {
+      atomicExch(err, kDevTimeoutTree);
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// 3-D tiled TMA load (x = K byte offset, y = row, z = modulus plane) into this
+// CTA's shared memory; completion counted on `bar`
+__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  // start >> 4 | LBO 16 B (unused for swizzled K-major) | SBO 1024 B (8-row
+  // groups) | version 1 | base offset 0 | SWIZZLE_128B
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+// kind::i8 instruction descriptor: D S32 (bits 4-5 = 2), A S8 (bits 7-9 = 1),
+// B S8 (bits 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at 24-28
+constexpr int kOzMmaM = 128, kOzMmaN = 256;
+constexpr uint32_t kOzIdesc = (2u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(kOzMmaN >> 3) << 17) | ((uint32_t)(kOzMmaM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(kOzIdesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// ----------------------------------------------------------- int8 GEMM
+constexpr int kOzBM = 256, kOzBN = 256, kOzBK = 128;  // K per stage in bytes (= elements)
+constexpr int kOzStages = 3;
+constexpr int kOzTile = kOzBM * kOzBK;                // 32 KB per operand tile
+constexpr uint32_t kOzStageBytes = 2 * kOzTile;
+constexpr int kOzThreads = 128;
+constexpr int kOzSmem = kOzStages * (int)kOzStageBytes + 1024 + 256;
+constexpr int kOzGroup = 8;  // tile rows per rasterisation group (L2 reuse)
+
+struct OzGemmArgs {
+  long M, N, K;
+  int tiles_m, tiles_n;
+  int lower;           // only tiles with tile row >= tile column
+  uint8_t* R;          // residue planes: R[l * plane + m + n * ldr]
+  long ldr, plane;
+  int p[kOzMaxMod];
+  unsigned magic[kOzMaxMod];
+  int* err;
+};
+
+__device__ __forceinline__ void tile_coords(const OzGemmArgs& a, long t, int& bm, int& bn) {
+  if (a.lower) {  // t -> (bm >= bn), t = bm (bm + 1) / 2 + bn
+    long i = (long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > t) --i;
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    bm = (int)i;
+    bn = (int)(t - i * (i + 1) / 2);
+    return;
+  }
+  // groups of kOzGroup tile rows, column-major inside a group
+  const long per = (long)kOzGroup * a.tiles_n;
+  const long g = t / per, r = t % per;
+  const long left = a.tiles_m - g * kOzGroup;
+  const int rows = (int)(left < kOzGroup ? left : kOzGroup);
+  bm = (int)(g * kOzGroup + r % rows);
+  bn = (int)(r / rows);
+}
+
+__global__ void __launch_bounds__(kOzThreads, 1)
+    oz_imma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                   const OzGemmArgs a) {
+  extern __shared__ __align__(1024) uint8_t osm[];
+  uint8_t* stages = osm + ((1024u - (smem_u32(osm) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kOzStages * kOzStageBytes);
+  uint64_t* empty = full + kOzStages;
+  uint64_t* done = empty + kOzStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int l = blockIdx.y;
+  int bm, bn;
+  tile_coords(a, blockIdx.x, bm, bn);
+  const long m0 = (long)bm * kOzBM, n0 = (long)bn * kOzBN;
+  const long nk = (a.K + kOzBK - 1) / kOzBK;
+
+  if (tid == 0) {
+    for (int s = 0; s < kOzStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     smem_u32(tslot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {  // TMA producer
+      for (long kb = 0; kb < nk; ++kb) {
+        const int s = (int)(kb % kOzStages);
+        if (kb >= kOzStages &&
+            !mbar_wait(empty + s, (uint32_t)((kb / kOzStages - 1) & 1), a.err)) {
+          ok = false;
+          break;
+        }
+        uint8_t* sa = stages + s * kOzStageBytes;
+        mbar_expect_tx(full + s, kOzStageBytes);
+        tma_load3(sa, &mapA, (int)(kb * kOzBK), (int)m0, l, full + s);
+        tma_load3(sa + kOzTile, &mapB, (int)(kb * kOzBK), (int)n0, l, full + s);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      for (long kb = 0; kb < nk; ++kb) {
+        const int s = (int)(kb % kOzStages);
+        if (!mbar_wait(full + s, (uint32_t)((kb / kOzStages) & 1), a.err)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t sa = smem_u32(stages + s * kOzStageBytes);
+        const uint32_t sb = sa + kOzTile;
+#pragma unroll
+        for (int ks = 0; ks < kOzBK / 32; ++ks) {
+          const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
+          const uint64_t db = smem_desc_sw128(sb + ks * 32);
+          umma_i8(tmem, smem_desc_sw128(sa + ks * 32), db, acc);
+          umma_i8(tmem + kOzMmaN, smem_desc_sw128(sa + kOzTile / 2 + ks * 32), db, acc);
+        }
+        umma_commit(empty + s);
+      }
+      umma_commit(done);  // fires when every MMA issued above has completed
+    }
+    __syncwarp();
+  }
+  const bool fin = mbar_wait(done, 0, a.err);
+  ok = __syncthreads_and(ok && fin);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    // epilogue: warp w reads TMEM lanes 32w..32w+31 = tile rows 32w + lane
+    // (accumulator 0) and 128 + 32w + lane (accumulator 1)
+    const int p = a.p[l];
+    const unsigned magic = a.magic[l];
+    // |acc| <= K 2^14 <= 2^30 < p 2^23 (K <= 2^16, p >= 173): acc + off is in
+    // [0, 2^32) and congruent to acc mod p
+    const unsigned off = (unsigned)p << 23;
+    uint8_t* R = a.R + (long)l * a.plane;
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const long gm = m0 + h * 128 + warp * 32 + lane;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kOzBN; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * kOzMmaN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(addr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (gm < a.M) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const long gn = n0 + c0 + j;
+            if (gn < a.N) {
+              const unsigned x = v[j] + off;
+              unsigned r = x - __umulhi(x, magic) * (unsigned)p;  // in [0, 2p)
+              if (r >= (unsigned)p) r -= (unsigned)p;
+              R[gm + gn * a.ldr] = (uint8_t)r;
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+}
+
+// ------------------------------------------------------------ quantisation
+// Row r of the operand = column r of S (K contiguous): 2-norm, exponent
+// e_r = P - ceil(log2 ||row||) (0 for a zero row), integers rint(S 2^e_r) and
+// their residues mod every p_l (symmetric range) as int8 into
+// Q[l * plane + r * ldq + k].  One block per row, 4 elements per thread.
+__global__ void oz_quant_kernel(long rows, long K, const double* __restrict__ S, long lds,
+                                int8_t* __restrict__ Q, long ldq, long plane, int* __restrict__ ex,
+                                const OzConsts c) {
+  __shared__ double red[32];
+  __shared__ double sscale;
+  for (long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const double* col = S + r * lds;
+    double ss = 0.0;
+    for (long k = threadIdx.x; k < K; k += blockDim.x) ss = fma(col[k], col[k], ss);
+    ss = warp_sum(ss);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+      int e = 0;
+      if (t > 0.0) {
+        int E;
+        frexp(sqrt(t), &E);  // ||row|| < 2^E
+        e = c.P - E;
+      }
+      ex[r] = e;
+      sscale = ldexp(1.0, e);
+    }
+    __syncthreads();
+    const double scale = sscale;
+    for (long k0 = 4 * (long)threadIdx.x; k0 < K; k0 += 4 * (long)blockDim.x) {
+      double v[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) v[q] = (k0 + q < K) ? rint(col[k0 + q] * scale) : 0.0;
+      for (int li = 0; li < c.nmod; ++li) {
+        const double p = (double)c.p[li];
+        const int half = (c.p[li] + 1) >> 1;
+        char4 o;
+        int8_t* ob = reinterpret_cast<int8_t*>(&o);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          double rr = fma(-floor(v[q] * c.invp[li]), p, v[q]);
+          if (rr < 0.0) rr += p;
+          if (rr >= p) rr -= p;
+          int ri = (int)rr;
+          if (ri >= half) ri -= c.p[li];
+          ob[q] = (int8_t)ri;
+        }
+        int8_t* dst = Q + (long)li * plane + r * ldq + k0;
+        if (k0 + 3 < K) {
+          *reinterpret_cast<char4*>(dst) = o;
+        } else {
+          for (int q = 0; q < 4 && k0 + q < K; ++q) dst[q] = ob[q];
+        }
+      }
+    }
+    __syncthreads();  // red / sscale reused by the next row
+  }
+}
+
+// B = A^T (FP64, column-major, m x n -> n x m), 32 x 32 tiles
+__global__ void oz_transpose_kernel(long m, long n, const double* __restrict__ A, long lda,
+                                    double* __restrict__ B, long ldb) {
+  __shared__ double t[32][33];
+  const long i0 = (long)blockIdx.x * 32, j0 = (long)blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long i = i0 + threadIdx.x, j = j0 + r;
+    t[r][threadIdx.x] = (i < m && j < n) ? A[i + j * lda] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long j = j0 + threadIdx.x, i = i0 + r;  // B(j, i) = A(i, j)
+    if (i < m && j < n) B[j + i * ldb] = t[threadIdx.x][r];
+  }
+}
+
+// --------------------------------------------------------------- CRT
+__device__ __forceinline__ double crt_value(const uint8_t* __restrict__ R, long plane, long idx,
+                                            const OzConsts& c) {
+  u128 s = 0;
+  for (int li = 0; li < c.nmod; ++li) {
+    const unsigned long long r = R[li * plane + idx];
+    s += (u128)r * mk128(c.wlo[li], c.whi[li]);
+  }
+  const u128 M = mk128(c.mlo, c.mhi);
+  const double sd = (double)(unsigned long long)(s >> 64) * 18446744073709551616.0 +
+                    (double)(unsigned long long)s;
+  unsigned long long q = (unsigned long long)(sd * c.invM);
+  u128 qm = (u128)q * M;
+  while (qm > s) {
+    qm -= M;
+    --q;
+  }
+  u128 x = s - qm;
+  while (x >= M) x -= M;
+  if (x > (M >> 1)) {
+    const u128 y = M - x;
+    return -((double)(unsigned long long)(y >> 64) * 18446744073709551616.0 +
+             (double)(unsigned long long)y);
+  }
+  return (double)(unsigned long long)(x >> 64) * 18446744073709551616.0 +
+         (double)(unsigned long long)x;
+}
+
+// D(m, n) = alpha 2^-(ea_m + eb_n) crt(m, n) + beta C(m, n) + diag [m == n].
+// lower: only m >= n is rebuilt and D(n, m) receives the same value (a
+// symmetric product).  32 x 32 tiles (threads 32 x 8); the mirrored writes go
+// through shared memory so that both stores are coalesced.
+__global__ void oz_crt_kernel(long M, long N, const uint8_t* __restrict__ R, long ldr, long plane,
+                              const int* __restrict__ ea, const int* __restrict__ eb, double alpha,
+                              double beta, const double* C, long ldc, double diag, double* D,
+                              long ldd, int lower, const OzConsts c) {
+  __shared__ double t[32][33];
+  const long i0 = (long)blockIdx.x * 32, j0 = (long)blockIdx.y * 32;
+  if (lower && j0 > i0) return;
+  const long i = i0 + threadIdx.x;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long j = j0 + r;
+    double out = 0.0;
+    const bool in = i < M && j < N && (!lower || i >= j);
+    if (in) {
+      const double v = crt_value(R, plane, i + j * ldr, c);
+      out = alpha * ldexp(v, -(ea[i] + eb[j]));
+      if (beta != 0.0) out = fma(beta, C[i + j * ldc], out);
+      if (i == j) out += diag;
+      D[i + j * ldd] = out;
+    }
+    t[r][threadIdx.x] = out;
+  }
+  if (!lower) return;
+  __syncthreads();
+  // mirror: D(j, i) for i > j, rows j0 + tx
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long ii = i0 + r, jj = j0 + threadIdx.x;  // element (ii, jj) computed above, ii >= jj
+    if (ii < M && jj < N && ii > jj) D[jj + ii * ldd] = t[threadIdx.x][r];
+  }
+}
+
+// D = beta C + diag I (the product vanishes); lower: both triangles from C's lower
+__global__ void oz_axpby_kernel(long M, long N, double beta, const double* C, long ldc, double diag,
+                                double* D, long ldd, int lower) {
+  const long i = (long)blockIdx.x * 32 + threadIdx.x;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const long j = (long)blockIdx.y * 32 + r;
+    if (i >= M || j >= N) continue;
+    const long si = (lower && i < j) ? j : i, sj = (lower && i < j) ? i : j;
+    double v = beta != 0.0 ? beta * C[si + sj * ldc] : 0.0;
+    if (i == j) v += diag;
+    D[i + j * ldd] = v;
+  }
+}
+
+// ------------------------------------------------------------ host side
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// planes of int8 rows (K bytes used of ld), `rows` rows per plane, nmod planes
+int make_plane_map(CUtensorMap* map, const int8_t* base, long rows, long K, long ld, long plane,
+                   int nmod) {
+  auto enc = encode_fn();
+  if (!enc) return EVD_ERR_CUDA;
+  cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nmod};
+  cuuint64_t strides[2] = {(cuuint64_t)ld, (cuuint64_t)plane};
+  cuuint32_t box[3] = {(cuuint32_t)kOzBK, (cuuint32_t)kOzBM, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)base, dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? EVD_SUCCESS : EVD_ERR_CUDA;
+}
+
+int* oz_err_word() {
+  static int* words[64] = {nullptr};
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+  if (!words[d]) {
+    int* p = nullptr;
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) return nullptr;
+    if (cudaMemset(p, 0, sizeof(int)) != cudaSuccess) return nullptr;
+    words[d] = p;
+  }
+  return words[d];
+}
+
+long al256(long x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+long oz_ld(long K) { return (K + 127) / 128 * 128; }
+
+OzLayout oz_layout(long M, long N, long K, int nmod, bool need_transpose) {
+  OzLayout L{};
+  const long ldq = oz_ld(K);
+  const long ldr = (M + 15) / 16 * 16;
+  long o = 0;
+  L.qa = o; o = al256(o + (long)nmod * M * ldq);
+  L.qb = o; o = al256(o + (long)nmod * N * ldq);
+  L.res = o; o = al256(o + (long)nmod * ldr * N);
+  L.ea = o; o = al256(o + 4 * M);
+  L.eb = o; o = al256(o + 4 * N);
+  L.tr = o; o = al256(o + (need_transpose ? 8 * std::max(M, N) * K : 0));
+  L.bytes = o + 256;
+  return L;
+}
+
+int oz_quantize(long rows, long K, const double* S, long lds, int8_t* Q, int* ex, int nmod,
+                cudaStream_t st) {
+  if (rows <= 0 || K <= 0) return EVD_SUCCESS;
+  const OzConsts c = make_consts(nmod, K);
+  const long ldq = oz_ld(K);
+  const long plane = rows * ldq;
+  const int blocks = (int)std::min<long>(rows, 8L * device_sm_count());
+  oz_quant_kernel<<<blocks, 256, 0, st>>>(rows, K, S, lds, Q, ldq, plane, ex, c);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+int oz_transpose(long m, long n, const double* A, long lda, double* B, long ldb,
+                 cudaStream_t st) {
+  if (m <= 0 || n <= 0) return EVD_SUCCESS;
+  oz_transpose_kernel<<<dim3(ceil_div_i(m, 32), ceil_div_i(n, 32)), dim3(32, 8), 0, st>>>(
+      m, n, A, lda, B, ldb);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t* Rz, int nmod,
+            bool lower, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return EVD_SUCCESS;
+  if (K <= 0 || K > kOzMaxK) return EVD_ERR_INVALID_ARG;  // INT32 accumulation bound
+  const long ldq = oz_ld(K);
+  CUtensorMap ma, mb;
+  EVD_TRY(make_plane_map(&ma, QA, M, K, ldq, M * ldq, nmod));
+  EVD_TRY(make_plane_map(&mb, QB, N, K, ldq, N * ldq, nmod));
+  const OzConsts c = make_consts(nmod, K);
+  OzGemmArgs a{};
+  a.M = M; a.N = N; a.K = K;
+  a.tiles_m = ceil_div_i(M, kOzBM);
+  a.tiles_n = ceil_div_i(N, kOzBN);
+  a.lower = lower ? 1 : 0;
+  a.R = Rz;
+  a.ldr = (M + 15) / 16 * 16;
+  a.plane = a.ldr * N;
+  for (int l = 0; l < nmod; ++l) {
+    a.p[l] = c.p[l];
+    a.magic[l] = c.magic[l];
+  }
+  a.err = oz_err_word();
+  if (!a.err) return EVD_ERR_CUDA;
+  const long tiles = lower ? (long)a.tiles_m * (a.tiles_m + 1) / 2 : (long)a.tiles_m * a.tiles_n;
+  if (tiles >= (1L << 31) || nmod > 65535) return EVD_ERR_INVALID_ARG;
+  EVD_TRY(smem_attr_once((const void*)oz_imma_kernel, kOzSmem));
+  oz_imma_kernel<<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, kOzSmem, st>>>(ma, mb, a);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+int oz_crt(long M, long N, long K, const uint8_t* Rz, const int* ea, const int* eb, int nmod,
+           double alpha, double beta, const double* C, long ldc, double diag, double* D, long ldd,
+           bool lower, cudaStream_t st) {
+  if (M <= 0 || N <= 0) return EVD_SUCCESS;
+  const OzConsts c = make_consts(nmod, K);
+  const long ldr = (M + 15) / 16 * 16;
+  oz_crt_kernel<<<dim3(ceil_div_i(M, 32), ceil_div_i(N, 32)), dim3(32, 8), 0, st>>>(
+      M, N, Rz, ldr, ldr * N, ea, eb, alpha, beta, C, ldc, diag, D, ldd, lower ? 1 : 0, c);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+int oz_check_err(cudaStream_t st) {
+  int* err = oz_err_word();
+  if (!err) return EVD_ERR_CUDA;
+  return read_device_error(err, st);
+}
+
+int oz_gemm(char ta, char tb, long M, long N, long K, double alpha, const double* A, long lda,
+            const double* B, long ldb, double beta, const double* C, long ldc, double diag,
+            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st) {
+  ta = (char)(ta | 0x20);
+  tb = (char)(tb | 0x20);
+  if ((ta != 'n' && ta != 't') || (tb != 'n' && tb != 't')) return EVD_ERR_INVALID_ARG;
+  if (M < 0 || N < 0 || K < 0 || nmod < kOzMinMod || nmod > kOzMaxMod) return EVD_ERR_INVALID_ARG;
+  if (lower && M != N) return EVD_ERR_INVALID_ARG;
+  if (M == 0 || N == 0) return EVD_SUCCESS;
+  if (!D || ldd < M || (beta != 0.0 && (!C || ldc < M))) return EVD_ERR_INVALID_ARG;
+  if (K == 0 || alpha == 0.0) {  // D = beta C + diag I
+    oz_axpby_kernel<<<dim3(ceil_div_i(M, 32), ceil_div_i(N, 32)), dim3(32, 8), 0, st>>>(
+        M, N, beta, C, ldc, diag, D, ldd, lower ? 1 : 0);
+    EVD_LAUNCHED();
+    return EVD_SUCCESS;
+  }
+  if (!A || !B || K > kOzMaxK) return EVD_ERR_INVALID_ARG;
+  if (lda < (ta == 't' ? K : M) || ldb < (tb == 't' ? N : K)) return EVD_ERR_INVALID_ARG;
+  const bool need_tr = (ta == 'n') || (tb == 't');
+  const OzLayout L = oz_layout(M, N, K, nmod, need_tr);
+  if (!work || lwork < L.bytes) return EVD_ERR_WORKSPACE;
+  uint8_t* base = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  int8_t* qa = reinterpret_cast<int8_t*>(base + L.qa);
+  int8_t* qb = reinterpret_cast<int8_t*>(base + L.qb);
+  uint8_t* rz = base + L.res;
+  int* ea = reinterpret_cast<int*>(base + L.ea);
+  int* eb = reinterpret_cast<int*>(base + L.eb);
+  double* tr = reinterpret_cast<double*>(base + L.tr);
+  // rows of op(A) with K contiguous: columns of A when ta == 't', else of A^T
+  if (ta == 't') {
+    EVD_TRY(oz_quantize(M, K, A, lda, qa, ea, nmod, st));
+  } else {
+    EVD_TRY(oz_transpose(M, K, A, lda, tr, K, st));
+    EVD_TRY(oz_quantize(M, K, tr, K, qa, ea, nmod, st));
+  }
+  // columns of op(B) with K contiguous: columns of B when tb == 'n'
+  if (tb == 'n') {
+    EVD_TRY(oz_quantize(N, K, B, ldb, qb, eb, nmod, st));
+  } else {
+    EVD_TRY(oz_transpose(N, K, B, ldb, tr, K, st));
+    EVD_TRY(oz_quantize(N, K, tr, K, qb, eb, nmod, st));
+  }
+  EVD_TRY(oz_imma(M, N, K, qa, qb, rz, nmod, lower, st));
+  EVD_TRY(oz_crt(M, N, K, rz, ea, eb, nmod, alpha, beta, C, ldc, diag, D, ldd, lower, st));
+  return EVD_SUCCESS;
+}
+
+int oz_bits(int nmod, long K) {
+  if (nmod < kOzMinMod || nmod > kOzMaxMod || K <= 0) return 0;
+  return make_consts(nmod, K).P;
+}
+
+}  // namespace evd
+
+extern "C" long evd_dgemm_ozaki_work_size(char transa, char transb, long m, long n, long k,
+                                          int moduli) {
+  if (m < 0 || n < 0 || k < 0 || moduli < evd::kOzMinMod || moduli > evd::kOzMaxMod) return 0;
+  const char ta = (char)(transa | 0x20), tb = (char)(transb | 0x20);
+  return evd::oz_layout(m, n, k, moduli, ta == 'n' || tb == 't').bytes;
+}
+
+extern "C" int evd_dgemm_ozaki(char transa, char transb, long m, long n, long k, double alpha,
+                               const double* A, long lda, const double* B, long ldb, double beta,
+                               double* C, long ldc, int moduli, void* work, long lwork,
+                               cudaStream_t stream) {
+  try {
+    EVD_TRY(evd::oz_gemm(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0.0, C,
+                         ldc, moduli, false, work, lwork, stream));
+    return evd::oz_check_err(stream);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+extern "C" int evd_ozaki_bits(int moduli, long k) { return evd::oz_bits(moduli, k); }

@@ -1,0 +1,45 @@
+// Emulated FP64 products on the integer tensor cores (Ozaki scheme II); the
+// kernels and their description are in ozaki.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace evd {
+
+constexpr int kOzMinMod = 4;     // fewest moduli (about 14-bit operands)
+constexpr int kOzMaxMod = 20;    // most moduli
+constexpr int kOzFp64Mod = 14;   // moduli for FP64-level products (53-bit operands)
+constexpr long kOzMaxK = 65536;  // INT32 accumulation bound of the epilogue's reduction
+
+// Byte offsets of the pieces of an emulated product's workspace.
+struct OzLayout {
+  long qa, qb, res, ea, eb, tr, bytes;
+};
+
+long oz_ld(long K);  // row pitch (bytes) of a quantised operand: K rounded up to 128
+OzLayout oz_layout(long M, long N, long K, int nmod, bool need_transpose);
+// bits P of the integer operands for nmod moduli and inner dimension K
+int oz_bits(int nmod, long K);
+
+// Rows of the operand = the `rows` columns of S (K long, column-major, lds):
+// exponents into ex[rows], residues into Q (nmod planes of rows x oz_ld(K)).
+int oz_quantize(long rows, long K, const double* S, long lds, int8_t* Q, int* ex, int nmod,
+                cudaStream_t st);
+// B = A^T (m x n column-major A)
+int oz_transpose(long m, long n, const double* A, long lda, double* B, long ldb, cudaStream_t st);
+// residue planes (M rounded up to 16) x N of (QA row m) . (QB row n) mod p_l
+int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t* R, int nmod,
+            bool lower, cudaStream_t st);
+// D = alpha 2^-(ea_m + eb_n) CRT(R) + beta C + diag I (lower: symmetric, mirrored)
+int oz_crt(long M, long N, long K, const uint8_t* R, const int* ea, const int* eb, int nmod,
+           double alpha, double beta, const double* C, long ldc, double diag, double* D, long ldd,
+           bool lower, cudaStream_t st);
+// the whole product: D = alpha op(A) op(B) + beta C + diag I
+int oz_gemm(char ta, char tb, long M, long N, long K, double alpha, const double* A, long lda,
+            const double* B, long ldb, double beta, const double* C, long ldc, double diag,
+            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st);
+// reads (and clears) the error word of the tensor-core waits; synchronises st
+int oz_check_err(cudaStream_t st);
+
+}  // namespace evd

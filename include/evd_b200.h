@@ -302,6 +302,25 @@ long evd_refine_syev_work_size(long n);
 int evd_refine_syev(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
                     double* work, long lwork, cudaStream_t stream);
 
+/* ---- Emulated FP64 products on the integer tensor cores ---------------- */
+
+/* Replaces the FP64 cuBLAS products of the reference's trailing update
+ * (api/TCblas/tc_ozimmu_syr2k.cu:54-192, cublasDgemm) with an Ozaki-II
+ * emulation: C = alpha op(A) op(B) + beta C, where every row of op(A) and
+ * column of op(B) is scaled to integers of at most P bits (2-norm), the
+ * product is formed exactly modulo `moduli` pairwise coprime numbers <= 256 by
+ * tcgen05 kind::i8 GEMMs with INT32 accumulation, and rebuilt by the Chinese
+ * remainder theorem.  Error <= ~sqrt(k) 2^-P ||row_i(op A)|| ||col_j(op B)||;
+ * P = evd_ozaki_bits(moduli, k) (53 for 14 moduli).  4 <= moduli <= 20,
+ * k <= 65536; C must not alias A or B.  work: evd_dgemm_ozaki_work_size
+ * bytes (moduli x (m + n + m n) k-ish bytes).  Synchronises `stream` (reads
+ * the error word of the bounded tensor-core waits). */
+long evd_dgemm_ozaki_work_size(char transa, char transb, long m, long n, long k, int moduli);
+int evd_dgemm_ozaki(char transa, char transb, long m, long n, long k, double alpha,
+                    const double* A, long lda, const double* B, long ldb, double beta, double* C,
+                    long ldc, int moduli, void* work, long lwork_bytes, cudaStream_t stream);
+int evd_ozaki_bits(int moduli, long k);
+
 /* ---- FP32 / FP16 entry points of the reference's API -------------------- */
 
 /* The reference instantiates panelQR and tc_ozimmu_syr2k for float and half
