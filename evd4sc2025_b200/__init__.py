@@ -42,7 +42,7 @@ __all__ = [
     "tsqr", "panel_qr", "sy2sb", "stedc", "bc_back", "bc_back_apply", "wy_from_slide",
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
     "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work", "dgemm_ozaki",
-    "dgemm_ozaki_work_size", "ozaki_bits",
+    "dgemm_ozaki_work_size", "ozaki_bits", "refine_syev_ozaki", "refine_ozaki_work",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -459,6 +459,32 @@ def refine_syev(A: torch.Tensor, X: torch.Tensor, iters: int = 2, w: torch.Tenso
     pa, lda = _cm(A, "A")
     px, ldx = _cm(X, "X")
     call("evd_refine_syev", n, pa, lda, _ptr(w), px, ldx, iters, _ptr(work), nw, _stream(stream))
+    return w, X
+
+
+def refine_ozaki_work(n: int, moduli: int = 14, device="cuda") -> torch.Tensor:
+    """Workspace (bytes) of :func:`refine_syev_ozaki` for order n."""
+    nb = int(lib().evd_refine_syev_ozaki_work_size(n, moduli))
+    if nb <= 0:
+        raise EvdError("evd_refine_syev_ozaki_work_size", -1)
+    return torch.empty(nb, dtype=torch.uint8, device=device)
+
+
+def refine_syev_ozaki(A: torch.Tensor, X: torch.Tensor, iters: int = 2, moduli: int = 14,
+                      moduli_update: int = 14, w: torch.Tensor | None = None, stream=None,
+                      work: torch.Tensor | None = None):
+    """Ogita-Aishima refinement (in place) with every product emulated on the
+    integer tensor cores: A X, X^T X and X^T A X with ``moduli`` moduli, the
+    update X E with ``moduli_update``.  Returns (w, X)."""
+    n = A.shape[0]
+    if work is None:
+        work = refine_ozaki_work(n, moduli, A.device)
+    if w is None:
+        w = torch.empty(n, dtype=F64, device=A.device)
+    pa, lda = _cm(A, "A")
+    px, ldx = _cm(X, "X")
+    call("evd_refine_syev_ozaki", n, pa, lda, _ptr(w), px, ldx, iters, moduli, moduli_update,
+         _ptr(work), work.numel(), _stream(stream))
     return w, X
 
 

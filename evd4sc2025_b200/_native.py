@@ -59,6 +59,8 @@ SIGNATURES = {
     "evd_syevd_batched": (_i, [_l, _p, _p, _p, _p, _p, _p, _i, _p, _l, _p]),
     "evd_refine_syev_work_size": (_l, [_l]),
     "evd_refine_syev": (_i, [_l, _p, _l, _p, _p, _l, _i, _p, _l, _p]),
+    "evd_refine_syev_ozaki_work_size": (_l, [_l, _i]),
+    "evd_refine_syev_ozaki": (_i, [_l, _p, _l, _p, _p, _l, _i, _i, _i, _p, _l, _p]),
     "evd_dgemm_ozaki_work_size": (_l, [_c, _c, _l, _l, _l, _i]),
     "evd_dgemm_ozaki": (_i, [_c, _c, _l, _l, _l, _d, _p, _l, _p, _l, _d, _p, _l, _i, _p, _l, _p]),
     "evd_ozaki_bits": (_i, [_i, _l]),

@@ -21,6 +21,7 @@
 
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 
 namespace evd {
 
@@ -157,9 +158,120 @@ __global__ void correction_kernel(long n, const double* __restrict__ S, long lds
   }
 }
 
+// The per-iteration steps after the products: eigenvalue estimates, norm
+// estimates by power iteration, the cluster threshold and the correction E
+// (into R).  S must be symmetric or is symmetrised; R holds -X^T X on entry.
+int refine_middle(long n, const double* S, double* R, double* lam, double* v0, double* v1,
+                  double* y0, double* y1, double* scal, cudaStream_t st) {
+  const int threads = 256;
+  const int gblocks = (int)std::min<long>(ceil_div_i(n, threads), 1024);
+  const int wblocks = (int)std::min<long>(ceil_div_i(n, threads / 32), 4096);
+  EVD_CUDA_TRY(cudaMemsetAsync(scal, 0, sizeof(double) * 32, st));
+  lambda_kernel<<<gblocks, threads, 0, st>>>(n, S, n, R, n, lam, v0, v1, scal);
+  EVD_LAUNCHED();
+  for (int p = 0; p < kPowerSteps; ++p) {
+    symv_kernel<<<wblocks, threads, 0, st>>>(n, S, n, lam, v0, y0, 1);
+    EVD_LAUNCHED();
+    normalize_kernel<<<1, 1024, 0, st>>>(n, y0, v0, scal + 4);
+    EVD_LAUNCHED();
+    symv_kernel<<<wblocks, threads, 0, st>>>(n, R, n, lam, v1, y1, 0);
+    EVD_LAUNCHED();
+    normalize_kernel<<<1, 1024, 0, st>>>(n, y1, v1, scal + 5);
+    EVD_LAUNCHED();
+  }
+  delta_kernel<<<1, 1, 0, st>>>(scal, n);
+  EVD_LAUNCHED();
+  const unsigned tiles = (unsigned)((n + 31) / 32);
+  correction_kernel<<<dim3(tiles, tiles), dim3(32, 8), 0, st>>>(n, S, n, R, n, lam, scal);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+// Workspace of the emulated-product refinement (bytes): the FP64 part of the
+// DMMA version (3 n^2 + O(n) doubles) plus three quantised operands of
+// `moduli` planes of n x ld bytes, the residue planes and the exponents.
+struct OzRefineLayout {
+  size_t f64, qa, qx, qp, res, ea, ex, ep, end;
+};
+
+OzRefineLayout oz_refine_layout(long n, int moduli) {
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  OzRefineLayout L{};
+  const size_t planes = (size_t)moduli * n * oz_ld(n);
+  size_t o = 0;
+  L.f64 = o; o = al(o + 8 * refine_layout(n).end);
+  L.qa = o; o = al(o + planes);
+  L.qx = o; o = al(o + planes);
+  L.qp = o; o = al(o + planes);
+  L.res = o; o = al(o + (size_t)moduli * ((n + 15) / 16 * 16) * n);
+  L.ea = o; o = al(o + 4 * n);
+  L.ex = o; o = al(o + 4 * n);
+  L.ep = o; o = al(o + 4 * n);
+  L.end = o + 256;
+  return L;
+}
+
 }  // namespace
 
 long refine_ws_doubles(long n) { return (long)refine_layout(n).end; }
+
+long refine_oz_ws_bytes(long n, int moduli) { return (long)oz_refine_layout(n, moduli).end; }
+
+// RefSyEv with every product emulated on the integer tensor cores:
+//   P = A X, R = -X^T X and S = X^T P with `moduli` moduli (14: FP64-level),
+//   X <- X + X E with `moduli_update` moduli (E is small, so fewer bits of
+//   it are needed for the same absolute accuracy).
+// X^T X and X^T P are symmetric: only their lower tiles are multiplied and
+// the CRT mirrors them.  A is quantised once for all iterations.
+int refine_syev_oz(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
+                   int moduli, int moduli_update, void* work, long lwork, cudaStream_t st) {
+  if (n < 0 || iters < 0) return EVD_ERR_INVALID_ARG;
+  if (n == 0 || iters == 0) return EVD_SUCCESS;
+  if (!A || !w || !X || !work || lda < n || ldX < n) return EVD_ERR_INVALID_ARG;
+  if (n > 65535 || moduli < kOzMinMod || moduli > kOzMaxMod || moduli_update < kOzMinMod ||
+      moduli_update > moduli)
+    return EVD_ERR_INVALID_ARG;
+  const OzRefineLayout L = oz_refine_layout(n, moduli);
+  if (lwork < (long)L.end) return EVD_ERR_WORKSPACE;
+  uint8_t* b8 = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  const RefineLayout F = refine_layout(n);
+  double* base = reinterpret_cast<double*>(b8 + L.f64);
+  double *P = base + F.AX, *S = base + F.S, *R = base + F.R, *lam = base + F.lam;
+  double *v0 = base + F.v0, *v1 = base + F.v1, *y0 = base + F.y0, *y1 = base + F.y1;
+  double* scal = base + F.scal;
+  int8_t* qa = reinterpret_cast<int8_t*>(b8 + L.qa);
+  int8_t* qx = reinterpret_cast<int8_t*>(b8 + L.qx);
+  int8_t* qp = reinterpret_cast<int8_t*>(b8 + L.qp);
+  uint8_t* res = b8 + L.res;
+  int* ea = reinterpret_cast<int*>(b8 + L.ea);
+  int* ex = reinterpret_cast<int*>(b8 + L.ex);
+  int* ep = reinterpret_cast<int*>(b8 + L.ep);
+  // rows of A = columns of A (symmetric)
+  EVD_TRY(oz_quantize(n, n, A, lda, qa, ea, moduli, st));
+  for (int it = 0; it < iters; ++it) {
+    EVD_TRY(oz_quantize(n, n, X, ldX, qx, ex, moduli, st));
+    // P = A X
+    EVD_TRY(oz_imma(n, n, n, qa, qx, res, moduli, false, st));
+    EVD_TRY(oz_crt(n, n, n, res, ea, ex, moduli, 1.0, 0.0, nullptr, n, 0.0, P, n, false, st));
+    // R = -X^T X (lower tiles, mirrored)
+    EVD_TRY(oz_imma(n, n, n, qx, qx, res, moduli, true, st));
+    EVD_TRY(oz_crt(n, n, n, res, ex, ex, moduli, -1.0, 0.0, nullptr, n, 0.0, R, n, true, st));
+    // S = X^T P (lower tiles, mirrored)
+    EVD_TRY(oz_quantize(n, n, P, n, qp, ep, moduli, st));
+    EVD_TRY(oz_imma(n, n, n, qx, qp, res, moduli, true, st));
+    EVD_TRY(oz_crt(n, n, n, res, ex, ep, moduli, 1.0, 0.0, nullptr, n, 0.0, S, n, true, st));
+    EVD_TRY(refine_middle(n, S, R, lam, v0, v1, y0, y1, scal, st));
+    // X <- X + X E: rows of X (through X^T in S, free now) and columns of E (in R)
+    EVD_TRY(oz_transpose(n, n, X, ldX, S, n, st));
+    EVD_TRY(oz_quantize(n, n, S, n, qp, ep, moduli_update, st));
+    EVD_TRY(oz_quantize(n, n, R, n, qx, ex, moduli_update, st));
+    EVD_TRY(oz_imma(n, n, n, qp, qx, res, moduli_update, false, st));
+    EVD_TRY(oz_crt(n, n, n, res, ep, ex, moduli_update, 1.0, 1.0, X, ldX, 0.0, X, ldX, false,
+                   st));
+  }
+  EVD_CUDA_TRY(cudaMemcpyAsync(w, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  return EVD_SUCCESS;
+}
 
 int refine_syev(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
                 double* work, long lwork, cudaStream_t st) {
@@ -173,31 +285,11 @@ int refine_syev(long n, const double* A, long lda, double* w, double* X, long ld
   double *AX = base + L.AX, *S = base + L.S, *R = base + L.R, *lam = base + L.lam;
   double *v0 = base + L.v0, *v1 = base + L.v1, *y0 = base + L.y0, *y1 = base + L.y1;
   double* scal = base + L.scal;
-  const int threads = 256;
-  const int gblocks = (int)std::min<long>(ceil_div_i(n, threads), 1024);
-  const int wblocks = (int)std::min<long>(ceil_div_i(n, threads / 32), 4096);
   for (int it = 0; it < iters; ++it) {
     EVD_TRY(dgemm('n', 'n', n, n, n, 1.0, A, lda, X, ldX, 0.0, AX, n, st));
     EVD_TRY(dgemm('t', 'n', n, n, n, 1.0, X, ldX, AX, n, 0.0, S, n, st));
     EVD_TRY(dgemm('t', 'n', n, n, n, -1.0, X, ldX, X, ldX, 0.0, R, n, st));
-    EVD_CUDA_TRY(cudaMemsetAsync(scal, 0, sizeof(double) * 32, st));
-    lambda_kernel<<<gblocks, threads, 0, st>>>(n, S, n, R, n, lam, v0, v1, scal);
-    EVD_LAUNCHED();
-    for (int p = 0; p < kPowerSteps; ++p) {
-      symv_kernel<<<wblocks, threads, 0, st>>>(n, S, n, lam, v0, y0, 1);
-      EVD_LAUNCHED();
-      normalize_kernel<<<1, 1024, 0, st>>>(n, y0, v0, scal + 4);
-      EVD_LAUNCHED();
-      symv_kernel<<<wblocks, threads, 0, st>>>(n, R, n, lam, v1, y1, 0);
-      EVD_LAUNCHED();
-      normalize_kernel<<<1, 1024, 0, st>>>(n, y1, v1, scal + 5);
-      EVD_LAUNCHED();
-    }
-    delta_kernel<<<1, 1, 0, st>>>(scal, n);
-    EVD_LAUNCHED();
-    const unsigned tiles = (unsigned)((n + 31) / 32);
-    correction_kernel<<<dim3(tiles, tiles), dim3(32, 8), 0, st>>>(n, S, n, R, n, lam, scal);
-    EVD_LAUNCHED();
+    EVD_TRY(refine_middle(n, S, R, lam, v0, v1, y0, y1, scal, st));
     // X <- X + X E (E in R; through AX, which is free now)
     EVD_TRY(copy_matrix(n, n, X, ldX, AX, n, st));
     EVD_TRY(dgemm('n', 'n', n, n, n, 1.0, X, ldX, R, n, 1.0, AX, n, st));
@@ -217,4 +309,21 @@ extern "C" long evd_refine_syev_work_size(long n) {
 extern "C" int evd_refine_syev(long n, const double* A, long lda, double* w, double* X, long ldX,
                                int iters, double* work, long lwork, cudaStream_t stream) {
   return evd::refine_syev(n, A, lda, w, X, ldX, iters, work, lwork, stream);
+}
+
+extern "C" long evd_refine_syev_ozaki_work_size(long n, int moduli) {
+  if (n < 0 || n > 65535 || moduli < evd::kOzMinMod || moduli > evd::kOzMaxMod) return 0;
+  return evd::refine_oz_ws_bytes(n, moduli);
+}
+
+extern "C" int evd_refine_syev_ozaki(long n, const double* A, long lda, double* w, double* X,
+                                     long ldX, int iters, int moduli, int moduli_update,
+                                     void* work, long lwork_bytes, cudaStream_t stream) {
+  try {
+    EVD_TRY(evd::refine_syev_oz(n, A, lda, w, X, ldX, iters, moduli, moduli_update, work,
+                                lwork_bytes, stream));
+    return evd::oz_check_err(stream);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
 }

@@ -302,6 +302,17 @@ long evd_refine_syev_work_size(long n);
 int evd_refine_syev(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
                     double* work, long lwork, cudaStream_t stream);
 
+/* The same iteration with every product emulated on the integer tensor cores
+ * (evd_dgemm_ozaki's scheme): A X, X^T X and X^T A X with `moduli` moduli (14:
+ * FP64-level operands), X E with `moduli_update` (<= moduli; E is of the size
+ * of X's error, so fewer bits of it give the same absolute accuracy).  The
+ * symmetric products multiply only their lower tiles.  n <= 65535; work:
+ * evd_refine_syev_ozaki_work_size(n, moduli) BYTES.  Synchronises `stream`. */
+long evd_refine_syev_ozaki_work_size(long n, int moduli);
+int evd_refine_syev_ozaki(long n, const double* A, long lda, double* w, double* X, long ldX,
+                          int iters, int moduli, int moduli_update, void* work,
+                          long lwork_bytes, cudaStream_t stream);
+
 /* ---- Emulated FP64 products on the integer tensor cores ---------------- */
 
 /* Replaces the FP64 cuBLAS products of the reference's trailing update

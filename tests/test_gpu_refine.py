@@ -1,6 +1,8 @@
-"""Ogita-Aishima refinement (evd_refine_syev) against LAPACK: FP32-accurate
-eigenpairs (LAPACK in FP32, or FP64 ones perturbed to 1e-6) are refined to
-the FP64 bars (eigenvalues 1e-12 ||A||, residual and orthogonality 1e-13)."""
+"""Ogita-Aishima refinement against LAPACK, with FP64 DMMA products
+(evd_refine_syev) and with emulated FP64 products on the integer tensor cores
+(evd_refine_syev_ozaki): FP32-accurate eigenpairs (LAPACK in FP32, or FP64
+ones perturbed to 1e-6) are refined to the FP64 bars (eigenvalues
+1e-12 ||A||, residual and orthogonality 1e-13)."""
 import numpy as np
 import pytest
 import torch
@@ -8,6 +10,11 @@ import torch
 from oracle import algos as O
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=["dmma", "ozaki"])
+def impl(request):
+    return request.param
 
 
 def _fp32_start(A):
@@ -22,28 +29,31 @@ def _metrics(A, w, X):
     return res, orth
 
 
-def _refine(cuda, evdlib, A, X0, iters):
+def _refine(cuda, evdlib, A, X0, iters, impl="dmma", moduli_update=14):
     Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
     Xd = evdlib.to_cm(torch.from_numpy(X0), device=cuda)
-    w, X = evdlib.refine_syev(Ad, Xd, iters)
+    if impl == "ozaki":
+        w, X = evdlib.refine_syev_ozaki(Ad, Xd, iters, moduli=14, moduli_update=moduli_update)
+    else:
+        w, X = evdlib.refine_syev(Ad, Xd, iters)
     torch.cuda.synchronize()
     return w.cpu().numpy(), X.cpu().numpy()
 
 
 @pytest.mark.parametrize("n", [64, 500, 1024])
-def test_refine_from_fp32(cuda, evdlib, n):
+def test_refine_from_fp32(cuda, evdlib, n, impl):
     A = O.sym_gaussian(n, seed=n + 17)
     X0 = _fp32_start(A)
     r0, o0 = _metrics(A, np.diag(X0.T @ A @ X0), X0)
     assert r0 > 1e-11 or o0 > 1e-11  # the start really is FP32-accurate only
-    w, X = _refine(cuda, evdlib, A, X0, 3)
+    w, X = _refine(cuda, evdlib, A, X0, 3, impl)
     res, orth = _metrics(A, w, X)
     assert res <= 1e-13 and orth <= 1e-13, (res, orth)
     assert np.abs(w - np.linalg.eigvalsh(A)).max() <= 1e-12 * np.linalg.norm(A, 2)
 
 
 @pytest.mark.parametrize("kind", ["geometric1e10", "uniform", "clustered"])
-def test_refine_known_spectrum(cuda, evdlib, kind):
+def test_refine_known_spectrum(cuda, evdlib, kind, impl):
     """uniform / clustered: from FP32 eigenpairs.  geometric1e10: eigenvalues
     down to 1e-10 ||A|| lie below FP32 resolution, so FP32 eigenvectors of
     that part are O(1) wrong and outside RefSyEv's convergence region (the
@@ -56,7 +66,7 @@ def test_refine_known_spectrum(cuda, evdlib, kind):
         X0 = Xe + 1e-8 * np.random.default_rng(2).standard_normal((n, n))
     else:
         X0 = _fp32_start(A)
-    w, X = _refine(cuda, evdlib, A, X0, 3)
+    w, X = _refine(cuda, evdlib, A, X0, 3, impl)
     res, orth = _metrics(A, w, X)
     assert res <= 1e-13 and orth <= 1e-13, (res, orth)
     order = np.argsort(w)
@@ -66,7 +76,7 @@ def test_refine_known_spectrum(cuda, evdlib, kind):
     assert np.abs(w[order] - np.sort(lam)).max() <= tol
 
 
-def test_refine_quadratic_convergence(cuda, evdlib):
+def test_refine_quadratic_convergence(cuda, evdlib, impl):
     n = 256
     A = O.sym_gaussian(n, seed=4)
     _, Xe = np.linalg.eigh(A)
@@ -74,28 +84,42 @@ def test_refine_quadratic_convergence(cuda, evdlib):
     X0 = Xe + 1e-6 * rng.standard_normal((n, n))
     errs = []
     for it in (1, 2):
-        w, X = _refine(cuda, evdlib, A, X0, it)
+        w, X = _refine(cuda, evdlib, A, X0, it, impl)
         s = np.sign(np.sum(X * Xe, axis=0))
         errs.append(np.abs(X * s - Xe).max())
     # quadratic: 1e-6 -> about 1e-12 times ||A|| / (smallest gap), then FP64 level
     assert errs[0] <= 1e-7 and errs[1] <= 1e-13, errs
 
 
-def test_refine_zero_iterations_and_empty(cuda, evdlib):
+def test_refine_zero_iterations_and_empty(cuda, evdlib, impl):
     A = O.sym_gaussian(32, seed=1)
     X0 = _fp32_start(A)
-    w, X = _refine(cuda, evdlib, A, X0, 0)
+    w, X = _refine(cuda, evdlib, A, X0, 0, impl)
     assert np.array_equal(X, X0)
 
 
-def test_refine_matches_oracle(cuda, evdlib):
+def test_refine_matches_oracle(cuda, evdlib, impl):
     """The GPU iteration and the numpy restatement (exact norms instead of the
     power-iteration estimates) give the same refined eigenpairs to rounding."""
     n = 300
     A = O.sym_gaussian(n, seed=31)
     X0 = _fp32_start(A)
-    w, X = _refine(cuda, evdlib, A, X0, 2)
+    w, X = _refine(cuda, evdlib, A, X0, 2, impl)
     lam_o, X_o = O.refine_syev(A, X0, 2)
     nA = np.linalg.norm(A, 2)
     assert np.abs(w - lam_o).max() <= 1e-13 * nA
     assert np.abs(X - X_o).max() <= 1e-11
+
+
+@pytest.mark.parametrize("mu", [8, 10])
+def test_refine_ozaki_fewer_update_moduli(cuda, evdlib, mu):
+    """X E with fewer moduli: E is O(error of X), so its products need fewer
+    bits for the same absolute accuracy; from an FP32 start the bars are met
+    after three iterations."""
+    n = 700
+    A = O.sym_gaussian(n, seed=77)
+    X0 = _fp32_start(A)
+    w, X = _refine(cuda, evdlib, A, X0, 3, "ozaki", moduli_update=mu)
+    res, orth = _metrics(A, w, X)
+    assert res <= 1e-13 and orth <= 1e-13, (res, orth)
+    assert np.abs(w - np.linalg.eigvalsh(A)).max() <= 1e-12 * np.linalg.norm(A, 2)
