@@ -43,6 +43,7 @@ __all__ = [
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
     "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work", "dgemm_ozaki",
     "dgemm_ozaki_work_size", "ozaki_bits", "refine_syev_ozaki", "refine_ozaki_work",
+    "syevd_mixed", "MixedWorkspace", "last_refine_ms", "mixed_last_timings",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -414,6 +415,59 @@ def syevd(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | None = N
 
 
 myEVD = syevd
+
+
+class MixedWorkspace:
+    """Reusable device workspace for :func:`syevd_mixed`."""
+
+    def __init__(self, n: int, b: int = 32, nb: int = 1024, moduli: int = 14,
+                 refine_iters: int = 0, device="cuda"):
+        nbytes = lib().evd_syevd_mixed_work_size(n, b, nb, moduli, refine_iters)
+        if nbytes <= 0:
+            raise EvdError("evd_syevd_mixed_work_size", -1)
+        self.key = (n, b, nb, moduli, refine_iters)
+        self.nbytes = int(nbytes)
+        self.buf = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
+
+
+def syevd_mixed(A: torch.Tensor, b: int = 32, nb: int = 1024, moduli: int = 14,
+                refine_iters: int = 0, moduli_update: int = 14,
+                ws: MixedWorkspace | None = None, timed: bool = False, stream=None,
+                w: torch.Tensor | None = None, X: torch.Tensor | None = None):
+    """All eigenpairs of the symmetric FP64 matrix A by the mixed form of the
+    solve: the stage-1 trailing SYR2K and the stage-1 back transformation as
+    emulated products on the integer tensor cores with ``moduli`` moduli (14:
+    FP64-level), then ``refine_iters`` Ogita-Aishima iterations on emulated
+    FP64 products (X E with ``moduli_update``).  A is not modified."""
+    n = A.shape[0]
+    dev = A.device
+    if ws is None or ws.key != (n, b, nb, moduli, refine_iters):
+        ws = MixedWorkspace(n, b, nb, moduli, refine_iters, device=dev)
+    if w is None:
+        w = torch.empty(n, dtype=F64, device=dev)
+    if X is None:
+        X = empty_cm(n, n, device=dev)
+    pa, lda = _cm(A, "A")
+    px, ldx = _cm(X, "X")
+    call("evd_syevd_mixed", n, b, nb, pa, lda, _ptr(w), px, ldx, moduli, refine_iters,
+         moduli_update, _ptr(ws.buf), ws.nbytes, 1 if timed else 0, _stream(stream))
+    return w, X
+
+
+def mixed_last_timings() -> dict:
+    """Stage times (ms) of the last timed :func:`syevd_mixed` on this thread.
+    q1_formation and stage2_on_q1t run on a side stream beside the chase and
+    the divide and conquer; x_eq_qz includes waiting for them."""
+    out = (C.c_double * 8)()
+    lib().evd_syevd_mixed_last_timings(out)
+    keys = ("sy2sb", "bulge_chasing", "tridiagonal_dc", "q1_formation", "stage2_on_q1t",
+            "x_eq_qz", "refine", "total")
+    return {k: float(v) for k, v in zip(keys, out)}
+
+
+def last_refine_ms() -> float:
+    """Refinement time (ms) of the last timed :func:`syevd_mixed` on this thread."""
+    return float(lib().evd_syevd_last_refine_ms())
 
 
 def syevd_values(A: torch.Tensor, b: int = 32, nb: int = 1024, ws: Workspace | None = None,

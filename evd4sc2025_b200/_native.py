@@ -55,6 +55,10 @@ SIGNATURES = {
     "evd_stebz": (_i, [_l, _p, _p, _p, _p, _l, _p]),
     "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
+    "evd_syevd_mixed_work_size": (_l, [_l, _l, _l, _i, _i]),
+    "evd_syevd_mixed": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _i, _i, _p, _l, _i, _p]),
+    "evd_syevd_last_refine_ms": (_d, []),
+    "evd_syevd_mixed_last_timings": (None, [_p]),
     "evd_syevd_batched_work_size": (_l, [_l, _p, _i]),
     "evd_syevd_batched": (_i, [_l, _p, _p, _p, _p, _p, _p, _i, _p, _l, _p]),
     "evd_refine_syev_work_size": (_l, [_l]),

@@ -15,7 +15,8 @@
 //      one tcgen05 kind::i8 GEMM with INT32 accumulation (|sum| <= K 2^14 <
 //      2^31 for K < 2^17), and the epilogue stores (a . b) mod p_l as a byte;
 //   3. the Chinese remainder theorem rebuilds a_i . b_j in (-Mod/2, Mod/2)
-//      exactly (128-bit integers), which is scaled back by 2^-(e_i + f_j).
+//      exactly (40-bit limbs held in doubles), which is converted to a double
+//      and scaled back by 2^-(e_i + f_j).
 // The only rounding is step 1: |D_ij - (op(A) op(B))_ij| <= ~ sqrt(K) 2^-P
 // ||op(A)_i|| ||op(B)_j||.  14 moduli give P = 53 (FP64 inputs); fewer moduli
 // trade accuracy for speed (P ~ 4 N - 2).
@@ -43,24 +44,28 @@ namespace {
 // ------------------------------------------------------------------ moduli
 // 256 and odd pairwise coprime numbers below it, largest first (their prime
 // factors: 2; 3 5 17; 11 23; 251; 13 19; 241; 239; 233; 229; 227; 223; 7 31;
-// 211; 199; 197; 193; 191; 181; 179; 173).
-constexpr int kModTable[kOzMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
-                                      223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+// 211; 199; 197; 193).
+constexpr int kModTable[kOzMaxMod] = {256, 255, 253, 251, 247, 241, 239, 233,
+                                      229, 227, 223, 217, 211, 199, 197, 193};
 
 typedef unsigned __int128 u128;
+constexpr u128 kLimbMask = ((u128)1 << 40) - 1;
 
+// CRT constants are split into 40-bit limbs held exactly in doubles: a sum of
+// up to 20 products (residue < 2^8) x (limb < 2^40) stays below 2^53.
+constexpr int kOzLimbs = 4;  // Mod < 2^160 for 20 moduli
 struct OzConsts {
   int nmod;
   int p[kOzMaxMod];
   unsigned magic[kOzMaxMod];   // floor(2^32 / p): Barrett quotient estimate
   double invp[kOzMaxMod];      // 1 / p
-  unsigned long long wlo[kOzMaxMod], whi[kOzMaxMod];  // CRT weights (M / p) ((M / p)^-1 mod p)
-  unsigned long long mlo, mhi;  // Mod = prod p
-  double invM;                  // 1 / Mod
-  int P;                        // bits of the integer operands (row norm <= 2^P)
+  double wl[kOzLimbs][kOzMaxMod];  // CRT weights (M / p) ((M / p)^-1 mod p), 40-bit limbs
+  double ml[kOzLimbs];         // Mod, 40-bit limbs
+  double Md;                   // Mod (rounded)
+  double invM;                 // 1 / Mod
+  int P;                       // bits of the integer operands (row norm <= 2^P)
 };
 
-__host__ __device__ __forceinline__ u128 mk128(unsigned long long lo, unsigned long long hi) { return ((u128)hi << 64) | lo; }
 
 // modular inverse of a mod p (p <= 256, gcd = 1), by search
 int inv_mod(u128 a, int p) {
@@ -81,13 +86,14 @@ OzConsts make_consts(int nmod, long K) {
     c.magic[l] = (unsigned)(((unsigned long long)1 << 32) / (unsigned long long)p);
     c.invp[l] = 1.0 / (double)p;
     const u128 Mi = M / (u128)p;
-    const u128 w = Mi * (u128)inv_mod(Mi, p);  // < M: (M/p) * (p - 1) < M
-    c.wlo[l] = (unsigned long long)w;
-    c.whi[l] = (unsigned long long)(w >> 64);
+    const u128 w = Mi * (u128)inv_mod(Mi, p);  // < M: (M/p) * (p - 1) < M < 2^126
+    for (int i = 0; i < kOzLimbs; ++i) c.wl[i][l] = (double)((w >> (40 * i)) & kLimbMask);
   }
-  c.mlo = (unsigned long long)M;
-  c.mhi = (unsigned long long)(M >> 64);
-  const long double Md = (long double)c.mhi * 18446744073709551616.0L + (long double)c.mlo;
+  for (int i = 0; i < kOzLimbs; ++i) c.ml[i] = (double)((M >> (40 * i)) & kLimbMask);
+  const long double Md =
+      (long double)(unsigned long long)(M >> 64) * 18446744073709551616.0L +
+      (long double)(unsigned long long)M;
+  c.Md = (double)Md;
   c.invM = (double)(1.0L / Md);
   // largest P with (2^P + sqrt(K)/2)^2 < M/2 (the rounding of each element
   // adds at most 1/2, so a row's norm grows by at most sqrt(K)/2)
@@ -180,11 +186,13 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 
 // ----------------------------------------------------------- int8 GEMM
 constexpr int kOzBM = 256, kOzBN = 256, kOzBK = 128;  // K per stage in bytes (= elements)
-constexpr int kOzStages = 3;
 constexpr int kOzTile = kOzBM * kOzBK;                // 32 KB per operand tile
 constexpr uint32_t kOzStageBytes = 2 * kOzTile;
 constexpr int kOzThreads = 128;
-constexpr int kOzSmem = kOzStages * (int)kOzStageBytes + 1024 + 256;
+// 3 stages (198 KB) normally; 2 stages (130 KB) leave room for another
+// kernel's CTA on the same SM (the bulge chase, 33 KB, runs beside the
+// products that overlap it)
+constexpr int oz_smem(int stages) { return stages * (int)kOzStageBytes + 1024 + 256; }
 constexpr int kOzGroup = 8;  // tile rows per rasterisation group (L2 reuse)
 
 struct OzGemmArgs {
@@ -216,14 +224,15 @@ __device__ __forceinline__ void tile_coords(const OzGemmArgs& a, long t, int& bm
   bn = (int)(r / rows);
 }
 
+template <int STAGES>
 __global__ void __launch_bounds__(kOzThreads, 1)
     oz_imma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    const OzGemmArgs a) {
   extern __shared__ __align__(1024) uint8_t osm[];
   uint8_t* stages = osm + ((1024u - (smem_u32(osm) & 1023u)) & 1023u);
-  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kOzStages * kOzStageBytes);
-  uint64_t* empty = full + kOzStages;
-  uint64_t* done = empty + kOzStages;
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + STAGES * kOzStageBytes);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int l = blockIdx.y;
@@ -233,7 +242,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   const long nk = (a.K + kOzBK - 1) / kOzBK;
 
   if (tid == 0) {
-    for (int s = 0; s < kOzStages; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
@@ -257,9 +266,9 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   if (warp == 0) {
     if (lane == 0) {  // TMA producer
       for (long kb = 0; kb < nk; ++kb) {
-        const int s = (int)(kb % kOzStages);
-        if (kb >= kOzStages &&
-            !mbar_wait(empty + s, (uint32_t)((kb / kOzStages - 1) & 1), a.err)) {
+        const int s = (int)(kb % STAGES);
+        if (kb >= STAGES &&
+            !mbar_wait(empty + s, (uint32_t)((kb / STAGES - 1) & 1), a.err)) {
           ok = false;
           break;
         }
@@ -273,8 +282,8 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   } else if (warp == 1) {
     if (lane == 0) {  // MMA issuer
       for (long kb = 0; kb < nk; ++kb) {
-        const int s = (int)(kb % kOzStages);
-        if (!mbar_wait(full + s, (uint32_t)((kb / kOzStages) & 1), a.err)) {
+        const int s = (int)(kb % STAGES);
+        if (!mbar_wait(full + s, (uint32_t)((kb / STAGES) & 1), a.err)) {
           ok = false;
           break;
         }
@@ -420,31 +429,53 @@ __global__ void oz_transpose_kernel(long m, long n, const double* __restrict__ A
 }
 
 // --------------------------------------------------------------- CRT
+// Limb arithmetic of the reconstruction: a value is x3 2^120 + x2 2^80 +
+// x1 2^40 + x0 with every limb an integer held exactly in a double.
+// canonical: x0, x1, x2 in [0, 2^40), the sign in x3
+__device__ __forceinline__ void limbs_canon(double (&x)[kOzLimbs]) {
+#pragma unroll
+  for (int i = 0; i < kOzLimbs - 1; ++i) {
+    const double c = floor(x[i] * 0x1p-40);
+    x[i] = fma(-c, 0x1p40, x[i]);
+    x[i + 1] += c;
+  }
+}
+__device__ __forceinline__ double limbs_value(const double (&x)[kOzLimbs]) {
+  return fma(x[3], 0x1p120, fma(x[2], 0x1p80, fma(x[1], 0x1p40, x[0])));
+}
+
+// The integer in (-Mod/2, Mod/2) with residues R[l * plane + idx] as a double:
+// S = sum_l r_l w_l (limb sums exact), X = S - q Mod with q from a rounded
+// quotient, then the representative nearest zero (the product's bound keeps
+// the true value within Mod/4, far from the decision points), then the
+// magnitude's limbs summed from the top limb down (each step one rounding).
 __device__ __forceinline__ double crt_value(const uint8_t* __restrict__ R, long plane, long idx,
                                             const OzConsts& c) {
-  u128 s = 0;
+  double x[kOzLimbs] = {0.0, 0.0, 0.0, 0.0};
   for (int li = 0; li < c.nmod; ++li) {
-    const unsigned long long r = R[li * plane + idx];
-    s += (u128)r * mk128(c.wlo[li], c.whi[li]);
+    const double r = (double)R[li * plane + idx];
+#pragma unroll
+    for (int i = 0; i < kOzLimbs; ++i) x[i] = fma(r, c.wl[i][li], x[i]);
   }
-  const u128 M = mk128(c.mlo, c.mhi);
-  const double sd = (double)(unsigned long long)(s >> 64) * 18446744073709551616.0 +
-                    (double)(unsigned long long)s;
-  unsigned long long q = (unsigned long long)(sd * c.invM);
-  u128 qm = (u128)q * M;
-  while (qm > s) {
-    qm -= M;
-    --q;
+  const double q = floor(limbs_value(x) * c.invM);
+#pragma unroll
+  for (int i = 0; i < kOzLimbs; ++i) x[i] = fma(-q, c.ml[i], x[i]);
+  limbs_canon(x);
+  // X = v + k Mod with k in {-1, 0, 1, 2} and |v| < Mod/4: k = rint(X / Mod)
+  const double k = rint(limbs_value(x) * c.invM);
+  if (k != 0.0) {
+#pragma unroll
+    for (int i = 0; i < kOzLimbs; ++i) x[i] = fma(-k, c.ml[i], x[i]);
+    limbs_canon(x);
   }
-  u128 x = s - qm;
-  while (x >= M) x -= M;
-  if (x > (M >> 1)) {
-    const u128 y = M - x;
-    return -((double)(unsigned long long)(y >> 64) * 18446744073709551616.0 +
-             (double)(unsigned long long)y);
+  const bool neg = x[3] < 0.0;
+  if (neg) {
+#pragma unroll
+    for (int i = 0; i < kOzLimbs; ++i) x[i] = -x[i];
+    limbs_canon(x);
   }
-  return (double)(unsigned long long)(x >> 64) * 18446744073709551616.0 +
-         (double)(unsigned long long)x;
+  const double mag = fma(x[3], 0x1p120, fma(x[2], 0x1p80, fma(x[1], 0x1p40, x[0])));
+  return neg ? -mag : mag;
 }
 
 // D(m, n) = alpha 2^-(ea_m + eb_n) crt(m, n) + beta C(m, n) + diag [m == n].
@@ -583,7 +614,7 @@ int oz_transpose(long m, long n, const double* A, long lda, double* B, long ldb,
 }
 
 int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t* Rz, int nmod,
-            bool lower, cudaStream_t st) {
+            bool lower, cudaStream_t st, bool lean) {
   if (M <= 0 || N <= 0) return EVD_SUCCESS;
   if (K <= 0 || K > kOzMaxK) return EVD_ERR_INVALID_ARG;  // INT32 accumulation bound
   const long ldq = oz_ld(K);
@@ -607,8 +638,13 @@ int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t*
   if (!a.err) return EVD_ERR_CUDA;
   const long tiles = lower ? (long)a.tiles_m * (a.tiles_m + 1) / 2 : (long)a.tiles_m * a.tiles_n;
   if (tiles >= (1L << 31) || nmod > 65535) return EVD_ERR_INVALID_ARG;
-  EVD_TRY(smem_attr_once((const void*)oz_imma_kernel, kOzSmem));
-  oz_imma_kernel<<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, kOzSmem, st>>>(ma, mb, a);
+  if (lean) {
+    EVD_TRY(smem_attr_once((const void*)oz_imma_kernel<2>, oz_smem(2)));
+    oz_imma_kernel<2><<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, oz_smem(2), st>>>(ma, mb, a);
+  } else {
+    EVD_TRY(smem_attr_once((const void*)oz_imma_kernel<3>, oz_smem(3)));
+    oz_imma_kernel<3><<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, oz_smem(3), st>>>(ma, mb, a);
+  }
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
@@ -633,7 +669,8 @@ int oz_check_err(cudaStream_t st) {
 
 int oz_gemm(char ta, char tb, long M, long N, long K, double alpha, const double* A, long lda,
             const double* B, long ldb, double beta, const double* C, long ldc, double diag,
-            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st) {
+            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st,
+            bool lean) {
   ta = (char)(ta | 0x20);
   tb = (char)(tb | 0x20);
   if ((ta != 'n' && ta != 't') || (tb != 'n' && tb != 't')) return EVD_ERR_INVALID_ARG;
@@ -673,8 +710,54 @@ int oz_gemm(char ta, char tb, long M, long N, long K, double alpha, const double
     EVD_TRY(oz_transpose(N, K, B, ldb, tr, K, st));
     EVD_TRY(oz_quantize(N, K, tr, K, qb, eb, nmod, st));
   }
-  EVD_TRY(oz_imma(M, N, K, qa, qb, rz, nmod, lower, st));
+  EVD_TRY(oz_imma(M, N, K, qa, qb, rz, nmod, lower, st, lean));
   EVD_TRY(oz_crt(M, N, K, rz, ea, eb, nmod, alpha, beta, C, ldc, diag, D, ldd, lower, st));
+  return EVD_SUCCESS;
+}
+
+// C(lower, mirrored) = alpha (Y Z^T + Z Y^T) + beta C as ONE emulated product
+// [Y | Z] [Z | Y]^T (K = 2k): the rows of both operands are rows of Y and Z,
+// brought K-contiguous by transposes into the workspace.
+long oz_syr2k_ws_bytes(long n, long k, int nmod) {
+  const long K = 2 * k;
+  const long ldq = oz_ld(K);
+  long o = 0;
+  o = al256(o + 8 * K * n);                           // [Y | Z]^T
+  o = al256(o + 8 * K * n);                           // [Z | Y]^T
+  o = al256(o + (long)nmod * n * ldq);                // qa
+  o = al256(o + (long)nmod * n * ldq);                // qb
+  o = al256(o + (long)nmod * ((n + 15) / 16 * 16) * n);  // residues
+  o = al256(o + 4 * n);
+  o = al256(o + 4 * n);
+  return o + 256;
+}
+
+int oz_syr2k_lower(long n, long k, double alpha, const double* Y, long ldy, const double* Z,
+                   long ldz, double beta, double* C, long ldc, int nmod, void* work, long lwork,
+                   cudaStream_t st) {
+  if (n <= 0) return EVD_SUCCESS;
+  if (k <= 0 || 2 * k > kOzMaxK || nmod < kOzMinMod || nmod > kOzMaxMod)
+    return EVD_ERR_INVALID_ARG;
+  if (lwork < oz_syr2k_ws_bytes(n, k, nmod)) return EVD_ERR_WORKSPACE;
+  const long K = 2 * k;
+  const long ldq = oz_ld(K);
+  uint8_t* b = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  long o = 0;
+  double* t1 = reinterpret_cast<double*>(b + o); o = al256(o + 8 * K * n);
+  double* t2 = reinterpret_cast<double*>(b + o); o = al256(o + 8 * K * n);
+  int8_t* qa = reinterpret_cast<int8_t*>(b + o); o = al256(o + (long)nmod * n * ldq);
+  int8_t* qb = reinterpret_cast<int8_t*>(b + o); o = al256(o + (long)nmod * n * ldq);
+  uint8_t* rz = b + o; o = al256(o + (long)nmod * ((n + 15) / 16 * 16) * n);
+  int* ea = reinterpret_cast<int*>(b + o); o = al256(o + 4 * n);
+  int* eb = reinterpret_cast<int*>(b + o);
+  EVD_TRY(oz_transpose(n, k, Y, ldy, t1, K, st));
+  EVD_TRY(oz_transpose(n, k, Z, ldz, t1 + k, K, st));
+  EVD_TRY(oz_transpose(n, k, Z, ldz, t2, K, st));
+  EVD_TRY(oz_transpose(n, k, Y, ldy, t2 + k, K, st));
+  EVD_TRY(oz_quantize(n, K, t1, K, qa, ea, nmod, st));
+  EVD_TRY(oz_quantize(n, K, t2, K, qb, eb, nmod, st));
+  EVD_TRY(oz_imma(n, n, K, qa, qb, rz, nmod, true, st));
+  EVD_TRY(oz_crt(n, n, K, rz, ea, eb, nmod, alpha, beta, C, ldc, 0.0, C, ldc, true, st));
   return EVD_SUCCESS;
 }
 

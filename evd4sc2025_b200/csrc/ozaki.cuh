@@ -8,7 +8,7 @@
 namespace evd {
 
 constexpr int kOzMinMod = 4;     // fewest moduli (about 14-bit operands)
-constexpr int kOzMaxMod = 20;    // most moduli
+constexpr int kOzMaxMod = 16;    // most moduli (Mod < 2^126)
 constexpr int kOzFp64Mod = 14;   // moduli for FP64-level products (53-bit operands)
 constexpr long kOzMaxK = 65536;  // INT32 accumulation bound of the epilogue's reduction
 
@@ -29,8 +29,9 @@ int oz_quantize(long rows, long K, const double* S, long lds, int8_t* Q, int* ex
 // B = A^T (m x n column-major A)
 int oz_transpose(long m, long n, const double* A, long lda, double* B, long ldb, cudaStream_t st);
 // residue planes (M rounded up to 16) x N of (QA row m) . (QB row n) mod p_l
+// lean: the 2-stage pipeline (130 KB of shared memory instead of 198 KB)
 int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t* R, int nmod,
-            bool lower, cudaStream_t st);
+            bool lower, cudaStream_t st, bool lean = false);
 // D = alpha 2^-(ea_m + eb_n) CRT(R) + beta C + diag I (lower: symmetric, mirrored)
 int oz_crt(long M, long N, long K, const uint8_t* R, const int* ea, const int* eb, int nmod,
            double alpha, double beta, const double* C, long ldc, double diag, double* D, long ldd,
@@ -38,8 +39,22 @@ int oz_crt(long M, long N, long K, const uint8_t* R, const int* ea, const int* e
 // the whole product: D = alpha op(A) op(B) + beta C + diag I
 int oz_gemm(char ta, char tb, long M, long N, long K, double alpha, const double* A, long lda,
             const double* B, long ldb, double beta, const double* C, long ldc, double diag,
-            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st);
+            double* D, long ldd, int nmod, bool lower, void* work, long lwork, cudaStream_t st,
+            bool lean = false);
+// C(lower, mirrored) = alpha (Y Z^T + Z Y^T) + beta C, Y and Z n x k
+long oz_syr2k_ws_bytes(long n, long k, int nmod);
+int oz_syr2k_lower(long n, long k, double alpha, const double* Y, long ldy, const double* Z,
+                   long ldz, double beta, double* C, long ldc, int nmod, void* work, long lwork,
+                   cudaStream_t st);
 // reads (and clears) the error word of the tensor-core waits; synchronises st
 int oz_check_err(cudaStream_t st);
+
+// Emulated-product settings of a solve: moduli of the contractions and the
+// workspace they use (nullptr / 0: FP64 DMMA products).
+struct OzWork {
+  int nmod;
+  uint8_t* ws;
+  long bytes;
+};
 
 }  // namespace evd

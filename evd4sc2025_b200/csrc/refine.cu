@@ -189,17 +189,18 @@ int refine_middle(long n, const double* S, double* R, double* lam, double* v0, d
 
 // Workspace of the emulated-product refinement (bytes): the FP64 part of the
 // DMMA version (3 n^2 + O(n) doubles) plus three quantised operands of
-// `moduli` planes of n x ld bytes, the residue planes and the exponents.
+// `moduli` planes of n x ld bytes, the residue planes and the exponents
+// (`with_f64` = false: the integer part only, from offset 0).
 struct OzRefineLayout {
   size_t f64, qa, qx, qp, res, ea, ex, ep, end;
 };
 
-OzRefineLayout oz_refine_layout(long n, int moduli) {
+OzRefineLayout oz_refine_layout(long n, int moduli, bool with_f64 = true) {
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   OzRefineLayout L{};
   const size_t planes = (size_t)moduli * n * oz_ld(n);
   size_t o = 0;
-  L.f64 = o; o = al(o + 8 * refine_layout(n).end);
+  L.f64 = o; o = with_f64 ? al(o + 8 * refine_layout(n).end) : 0;
   L.qa = o; o = al(o + planes);
   L.qx = o; o = al(o + planes);
   L.qp = o; o = al(o + planes);
@@ -216,6 +217,9 @@ OzRefineLayout oz_refine_layout(long n, int moduli) {
 long refine_ws_doubles(long n) { return (long)refine_layout(n).end; }
 
 long refine_oz_ws_bytes(long n, int moduli) { return (long)oz_refine_layout(n, moduli).end; }
+long refine_oz_int_bytes(long n, int moduli) {
+  return (long)oz_refine_layout(n, moduli, false).end;
+}
 
 // RefSyEv with every product emulated on the integer tensor cores:
 //   P = A X, R = -X^T X and S = X^T P with `moduli` moduli (14: FP64-level),
@@ -223,19 +227,21 @@ long refine_oz_ws_bytes(long n, int moduli) { return (long)oz_refine_layout(n, m
 //   it are needed for the same absolute accuracy).
 // X^T X and X^T P are symmetric: only their lower tiles are multiplied and
 // the CRT mirrors them.  A is quantised once for all iterations.
-int refine_syev_oz(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
-                   int moduli, int moduli_update, void* work, long lwork, cudaStream_t st) {
+// f64: refine_ws_doubles(n) doubles; iwork: refine_oz_int_bytes(n, moduli)
+// bytes (256-byte aligned)
+int refine_syev_oz_split(long n, const double* A, long lda, double* w, double* X, long ldX,
+                         int iters, int moduli, int moduli_update, double* f64, uint8_t* iwork,
+                         cudaStream_t st) {
   if (n < 0 || iters < 0) return EVD_ERR_INVALID_ARG;
   if (n == 0 || iters == 0) return EVD_SUCCESS;
-  if (!A || !w || !X || !work || lda < n || ldX < n) return EVD_ERR_INVALID_ARG;
+  if (!A || !w || !X || !f64 || !iwork || lda < n || ldX < n) return EVD_ERR_INVALID_ARG;
   if (n > 65535 || moduli < kOzMinMod || moduli > kOzMaxMod || moduli_update < kOzMinMod ||
       moduli_update > moduli)
     return EVD_ERR_INVALID_ARG;
-  const OzRefineLayout L = oz_refine_layout(n, moduli);
-  if (lwork < (long)L.end) return EVD_ERR_WORKSPACE;
-  uint8_t* b8 = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  const OzRefineLayout L = oz_refine_layout(n, moduli, false);
+  uint8_t* b8 = iwork;
   const RefineLayout F = refine_layout(n);
-  double* base = reinterpret_cast<double*>(b8 + L.f64);
+  double* base = reinterpret_cast<double*>(((uintptr_t)f64 + 255) & ~(uintptr_t)255);
   double *P = base + F.AX, *S = base + F.S, *R = base + F.R, *lam = base + F.lam;
   double *v0 = base + F.v0, *v1 = base + F.v1, *y0 = base + F.y0, *y1 = base + F.y1;
   double* scal = base + F.scal;
@@ -297,6 +303,19 @@ int refine_syev(long n, const double* A, long lda, double* w, double* X, long ld
   }
   EVD_CUDA_TRY(cudaMemcpyAsync(w, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   return EVD_SUCCESS;
+}
+
+int refine_syev_oz(long n, const double* A, long lda, double* w, double* X, long ldX, int iters,
+                   int moduli, int moduli_update, void* work, long lwork, cudaStream_t st) {
+  if (n < 0 || iters < 0) return EVD_ERR_INVALID_ARG;
+  if (n == 0 || iters == 0) return EVD_SUCCESS;
+  if (n > 65535 || moduli < kOzMinMod || moduli > kOzMaxMod) return EVD_ERR_INVALID_ARG;
+  if (!work) return EVD_ERR_INVALID_ARG;
+  const OzRefineLayout L = oz_refine_layout(n, moduli);
+  if (lwork < (long)L.end) return EVD_ERR_WORKSPACE;
+  uint8_t* b8 = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  return refine_syev_oz_split(n, A, lda, w, X, ldX, iters, moduli, moduli_update,
+                              reinterpret_cast<double*>(b8 + L.f64), b8 + L.qa, st);
 }
 
 }  // namespace evd

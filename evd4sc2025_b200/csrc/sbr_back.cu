@@ -15,6 +15,7 @@
 // evd_q_from_wy:     computerQFromWY (api/computerQFromWY.cu:5-17).
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 
 namespace evd {
 
@@ -74,10 +75,19 @@ long sbr_back_ws_doubles(long n, long b, long nk) {
   return std::max(n * nk / 2, nk * n) + 64;
 }
 
-// X <- Q1 X using slab-merged W (call wy_merge_slabs first).
+// Emulated-product workspace of sbr_apply_slabs (bytes): the larger of its
+// two products' (T = Y_s^T X with K = rows, X -= W_s T with K = nk).
+long sbr_apply_oz_bytes(long n, long nk, long ncols, int nmod) {
+  return std::max(oz_layout(nk, ncols, n, nmod, false).bytes,
+                  oz_layout(n, ncols, nk, nmod, true).bytes);
+}
+
+// X <- Q1 X using slab-merged W (call wy_merge_slabs first).  oz != nullptr:
+// both products of every slab are emulated FP64 products on the integer
+// tensor cores.
 int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const double* dY,
                     long ldY, double* X, long ldX, long ncols, double* work, size_t work_n,
-                    cudaStream_t st) {
+                    cudaStream_t st, const OzWork* oz) {
   const long npcols = ((n - 1) / b) * b;  // panel columns (stage 1 leaves the last b-block)
   if (npcols <= 0 || ncols <= 0) return EVD_SUCCESS;
   const long nslabs = (npcols + nk - 1) / nk;
@@ -89,10 +99,54 @@ int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const d
     if (m <= 0 || w <= 0) continue;
     // T = Y_s^T X[r0:, :]  (w x ncols), then X[r0:, :] -= W_s T
     if ((size_t)(w * ncols) > work_n) return EVD_ERR_WORKSPACE;
+    if (oz) {
+      EVD_TRY(oz_gemm('t', 'n', w, ncols, m, 1.0, dY + r0 + c0 * ldY, ldY, X + r0, ldX, 0.0,
+                      nullptr, w, 0.0, work, w, oz->nmod, false, oz->ws, oz->bytes, st));
+      EVD_TRY(oz_gemm('n', 'n', m, ncols, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, X + r0,
+                      ldX, 0.0, X + r0, ldX, oz->nmod, false, oz->ws, oz->bytes, st));
+      continue;
+    }
     EVD_TRY(dgemm('t', 'n', w, ncols, m, 1.0, dY + r0 + c0 * ldY, ldY, X + r0, ldX, 0.0, work, w,
                   st));
     EVD_TRY(dgemm('n', 'n', m, ncols, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, X + r0,
                   ldX, st));
+  }
+  return EVD_SUCCESS;
+}
+
+// Q1 = prod_p (I - W_p Y_p^T) formed explicitly into M (slab-merged W, Y:
+// call wy_merge_slabs first).  M = I, then for the slabs last to first
+//   M[r0:, r0:] -= W_s (Y_s^T M[r0:, r0:])
+// where r0 is the slab's first row: outside rows and columns r0.. M is still
+// the identity, so the products shrink with the slab index and the whole
+// formation costs (4/3) n^3 flops instead of 2 n^3 (the reference forms Q1
+// from I the same way, src/EVD/myEVD.cu:213-233, over the full matrix).
+// oz != nullptr: emulated products (lean: the 2-stage integer GEMM, which
+// shares SMs with the bulge chase running beside it).
+int sbr_form_q1(long n, long b, long nk, const double* dW, long ldW, const double* dY, long ldY,
+                double* M, long ldM, double* work, size_t work_n, cudaStream_t st,
+                const OzWork* oz, bool lean) {
+  EVD_TRY(set_identity(n, n, M, ldM, st));
+  const long npcols = ((n - 1) / b) * b;
+  if (npcols <= 0) return EVD_SUCCESS;
+  const long nslabs = (npcols + nk - 1) / nk;
+  for (long s = nslabs - 1; s >= 0; --s) {
+    const long c0 = s * nk;
+    const long w = std::min(nk, npcols - c0);
+    const long r0 = c0 + b;
+    const long m = n - r0;
+    if (m <= 0 || w <= 0) continue;
+    if ((size_t)(w * m) > work_n) return EVD_ERR_WORKSPACE;
+    double* Mb = M + r0 + r0 * ldM;
+    if (oz) {
+      EVD_TRY(oz_gemm('t', 'n', w, m, m, 1.0, dY + r0 + c0 * ldY, ldY, Mb, ldM, 0.0, nullptr, w,
+                      0.0, work, w, oz->nmod, false, oz->ws, oz->bytes, st, lean));
+      EVD_TRY(oz_gemm('n', 'n', m, m, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, Mb, ldM,
+                      0.0, Mb, ldM, oz->nmod, false, oz->ws, oz->bytes, st, lean));
+    } else {
+      EVD_TRY(dgemm('t', 'n', w, m, m, 1.0, dY + r0 + c0 * ldY, ldY, Mb, ldM, 0.0, work, w, st));
+      EVD_TRY(dgemm('n', 'n', m, m, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, Mb, ldM, st));
+    }
   }
   return EVD_SUCCESS;
 }
@@ -118,7 +172,7 @@ extern "C" int evd_sbr_back(long n, long b, long nk, double* dW, long ldW, const
   const long npcols = ((n - 1) / b) * b;
   EVD_TRY(evd::wy_merge_slabs(n, b, nk, npcols, dW, ldW, dY, ldY, work, stream));
   return evd::sbr_apply_slabs(n, b, nk, dW, ldW, dY, ldY, X, ldX, ncols, work, (size_t)lwork,
-                              stream);
+                              stream, nullptr);
 }
 
 extern "C" int evd_wy_from_slide(long M, long N, long slideWidth, double* dW, long ldW,

@@ -23,6 +23,7 @@
 //  * skinny products (n = 32) use split-K with a deterministic reduction.
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 #include "panel_qr.cuh"
 
 namespace evd {
@@ -82,9 +83,11 @@ static Sy2sbLayout sy2sb_layout(long M, long b, long nb) {
 
 long sy2sb_ws_doubles(long M, long b, long nb) { return sy2sb_layout(M, b, nb).total; }
 
+// oz != nullptr: the trailing SYR2K is an emulated FP64 product on the
+// integer tensor cores (oz->nmod moduli) instead of the DMMA GEMM.
 int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, long ldA,
           double* dW, long ldW, double* dY, long ldY, double* dZ, long ldZ, double* dR, long ldR,
-          double* work, long lwork, cudaStream_t st) {
+          double* work, long lwork, cudaStream_t st, const OzWork* oz) {
   if (M <= 0) return EVD_SUCCESS;
   if (M != N || b != 32 || nb <= 0 || nb % b != 0 || M % nb != 0) return EVD_ERR_INVALID_ARG;
   if (ldOA < M || ldA < M || ldW < M || ldY < M || ldZ < M || ldR < M) return EVD_ERR_INVALID_ARG;
@@ -152,8 +155,13 @@ int sy2sb(long M, long N, long b, long nb, double* OA, long ldOA, double* dA, lo
     if (Nf - nb <= 0) break;
     // trailing update of the working copy (lower tiles, mirrored)
     const long t0 = off + nb;
-    EVD_TRY(syr2k_lower_mirror(Nf - nb, nb, -1.0, dY + t0 + off * ldY, ldY, dZ + nb, ldZ, 1.0,
-                               OA + t0 + t0 * ldOA, ldOA, st));
+    if (oz) {
+      EVD_TRY(oz_syr2k_lower(Nf - nb, nb, -1.0, dY + t0 + off * ldY, ldY, dZ + nb, ldZ, 1.0,
+                             OA + t0 + t0 * ldOA, ldOA, oz->nmod, oz->ws, oz->bytes, st));
+    } else {
+      EVD_TRY(syr2k_lower_mirror(Nf - nb, nb, -1.0, dY + t0 + off * ldY, ldY, dZ + nb, ldZ, 1.0,
+                                 OA + t0 + t0 * ldOA, ldOA, st));
+    }
   }
   // dA <- symmetric band (copyMatrixL2U, src/EVD/myEVD.cu:346)
   dim3 g2(ceil_div_i(M, 32), ceil_div_i(M, 32));
@@ -191,5 +199,5 @@ extern "C" int evd_sy2sb(long M, long N, long b, long nb, double* dOriA, long ld
                          long ldZ, double* dR, long ldR, double* work, long lwork,
                          cudaStream_t stream) {
   return evd::sy2sb(M, N, b, nb, dOriA, ldOriA, dA, ldA, dW, ldW, dY, ldY, dZ, ldZ, dR, ldR,
-                    work, lwork, stream);
+                    work, lwork, stream, nullptr);
 }

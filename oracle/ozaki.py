@@ -17,9 +17,9 @@ of residues:
 
 The GPU forms a_i . b_j modulo each p_l and rebuilds it by the Chinese
 remainder theorem; when |a_i . b_j| < Mod/2 (which the choice of P
-guarantees) the two agree exactly, and the conversion of the 128-bit integer to
-a double is the same (high and low 64-bit halves converted separately), so the
-results are bit-for-bit equal.
+guarantees) the two agree exactly, and the conversion of the integer to a
+double is the same (40-bit limbs summed from the top down), so the results are
+bit-for-bit equal.
 """
 from __future__ import annotations
 
@@ -27,8 +27,8 @@ import math
 
 import numpy as np
 
-MODULI = (256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
-          223, 217, 211, 199, 197, 193, 191, 181, 179, 173)
+MODULI = (256, 255, 253, 251, 247, 241, 239, 233,
+          229, 227, 223, 217, 211, 199, 197, 193)
 
 
 def modulus_product(nmod: int) -> int:
@@ -59,10 +59,14 @@ def quantize_rows(S: np.ndarray, P: int):
 
 
 def _to_double(x: int) -> float:
-    """Two-half conversion of |x| < 2^128 used by the device code."""
+    """The device's conversion of the rebuilt integer: the magnitude's 40-bit
+    limbs y3..y0 summed as y3 2^120 + (y2 2^80 + (y1 2^40 + y0)), one rounding
+    per addition (the products by powers of two are exact)."""
     neg = x < 0
     x = -x if neg else x
-    v = float(x >> 64) * 18446744073709551616.0 + float(x & 0xFFFFFFFFFFFFFFFF)
+    m = (1 << 40) - 1
+    y0, y1, y2, y3 = x & m, (x >> 40) & m, (x >> 80) & m, x >> 120
+    v = float(y3) * 2.0 ** 120 + (float(y2) * 2.0 ** 80 + (float(y1) * 2.0 ** 40 + float(y0)))
     return -v if neg else v
 
 

@@ -17,7 +17,7 @@ def test_moduli_pairwise_coprime():
             assert math.gcd(p, q) == 1
 
 
-@pytest.mark.parametrize("nmod", [4, 8, 14, 20])
+@pytest.mark.parametrize("nmod", [4, 8, 14, 16])
 def test_crt_round_trip(nmod):
     rng = np.random.default_rng(nmod)
     M = Z.modulus_product(nmod)
