@@ -21,14 +21,14 @@
 // ||op(A)_i|| ||op(B)_j||.  14 moduli give P = 53 (FP64 inputs); fewer moduli
 // trade accuracy for speed (P ~ 4 N - 2).
 //
-// The int8 GEMM (one launch for all moduli, blockIdx.y = modulus): CTA tile
-// 256 x 256 as two M128 N256 K32 tcgen05.mma per K step into two 256-column
-// INT32 accumulators in tensor memory (all 512 columns); both operands K-major
-// (rows of 128 bytes), brought in by TMA (cp.async.bulk.tensor, 128-byte
-// swizzle, this GPU's own memory only, no multicast) through a 3-stage
-// mbarrier pipeline: one thread issues the copies, one thread issues the
-// MMAs, and all four warps run the epilogue (tcgen05.ld, Barrett reduction,
-// byte stores).  Every wait is bounded (2 s) and reports EVD_ERR_TIMEOUT.
+// The int8 GEMM (one persistent launch for all moduli): tiles of 128 x 256 as
+// M128 N256 K32 tcgen05.mma into one of two 256-column INT32 accumulators in
+// tensor memory; both operands K-major (rows of 128 bytes), brought in by TMA
+// (cp.async.bulk.tensor, 128-byte swizzle, this GPU's own memory only, no
+// multicast) through a 4-stage mbarrier ring.  One thread issues the copies,
+// one thread the MMAs, and four warps drain the previous tile's accumulator
+// (tcgen05.ld, Barrett reduction, byte stores) while the next tile is being
+// multiplied.  Every wait is bounded (2 s) and reports EVD_ERR_TIMEOUT.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <math.h>
@@ -58,7 +58,8 @@ struct OzConsts {
   int nmod;
   int p[kOzMaxMod];
   unsigned magic[kOzMaxMod];   // floor(2^32 / p): Barrett quotient estimate
-  double invp[kOzMaxMod];      // 1 / p
+  int k16[kOzMaxMod], k32[kOzMaxMod], k48[kOzMaxMod];  // 2^16, 2^32, 2^48 mod p
+  int nlimb;                   // 40-bit limbs needed for Mod (3 up to 15 moduli)
   double wl[kOzLimbs][kOzMaxMod];  // CRT weights (M / p) ((M / p)^-1 mod p), 40-bit limbs
   double ml[kOzLimbs];         // Mod, 40-bit limbs
   double Md;                   // Mod (rounded)
@@ -84,12 +85,15 @@ OzConsts make_consts(int nmod, long K) {
     const int p = kModTable[l];
     c.p[l] = p;
     c.magic[l] = (unsigned)(((unsigned long long)1 << 32) / (unsigned long long)p);
-    c.invp[l] = 1.0 / (double)p;
+    c.k16[l] = (int)((1ull << 16) % (unsigned long long)p);
+    c.k32[l] = (int)((1ull << 32) % (unsigned long long)p);
+    c.k48[l] = (int)((1ull << 48) % (unsigned long long)p);
     const u128 Mi = M / (u128)p;
     const u128 w = Mi * (u128)inv_mod(Mi, p);  // < M: (M/p) * (p - 1) < M < 2^126
     for (int i = 0; i < kOzLimbs; ++i) c.wl[i][l] = (double)((w >> (40 * i)) & kLimbMask);
   }
   for (int i = 0; i < kOzLimbs; ++i) c.ml[i] = (double)((M >> (40 * i)) & kLimbMask);
+  c.nlimb = (M >> 120) == 0 ? 3 : 4;
   const long double Md =
       (long double)(unsigned long long)(M >> 64) * 18446744073709551616.0L +
       (long double)(unsigned long long)M;
@@ -185,20 +189,29 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 }
 
 // ----------------------------------------------------------- int8 GEMM
-constexpr int kOzBM = 256, kOzBN = 256, kOzBK = 128;  // K per stage in bytes (= elements)
-constexpr int kOzTile = kOzBM * kOzBK;                // 32 KB per operand tile
-constexpr uint32_t kOzStageBytes = 2 * kOzTile;
-constexpr int kOzThreads = 128;
-// 3 stages (198 KB) normally; 2 stages (130 KB) leave room for another
+// Persistent, warp-specialised: one CTA per SM walks the tiles t = blockIdx.x,
+// + gridDim.x, ... (modulus-major).  Warp 0 lane 0 issues the TMA copies of a
+// 4-stage (lean: 2-stage) shared-memory ring, warp 1 lane 0 issues the MMAs
+// into one of two 256-column INT32 accumulators in tensor memory (tile t into
+// buffer t & 1), and warps 2-5 drain the other buffer (tcgen05.ld, Barrett
+// reduction, byte stores) while the next tile is being multiplied.
+constexpr int kPM = 128, kPN = 256, kPK = 128;   // tile rows, columns, K bytes per stage
+constexpr uint32_t kPTileA = kPM * kPK;          // 16 KB
+constexpr uint32_t kPTileB = kPN * kPK;          // 32 KB
+constexpr uint32_t kPStage = kPTileA + kPTileB;  // 48 KB
+constexpr int kPThreads = 192;
+constexpr int kOzGroup = 8;                      // tile rows per rasterisation group (L2 reuse)
+// 4 stages (193 KB) normally; 2 stages (97 KB) leave room for another
 // kernel's CTA on the same SM (the bulge chase, 33 KB, runs beside the
 // products that overlap it)
-constexpr int oz_smem(int stages) { return stages * (int)kOzStageBytes + 1024 + 256; }
-constexpr int kOzGroup = 8;  // tile rows per rasterisation group (L2 reuse)
+constexpr int oz_smem(int stages) { return stages * (int)kPStage + 1024 + 256; }
 
 struct OzGemmArgs {
   long M, N, K;
   int tiles_m, tiles_n;
-  int lower;           // only tiles with tile row >= tile column
+  int lower;           // only tiles that meet the lower triangle (row >= column)
+  int nmod;
+  long tiles_per_mod;
   uint8_t* R;          // residue planes: R[l * plane + m + n * ldr]
   long ldr, plane;
   int p[kOzMaxMod];
@@ -206,13 +219,19 @@ struct OzGemmArgs {
   int* err;
 };
 
+// tile index inside one modulus plane -> (tile row, tile column)
 __device__ __forceinline__ void tile_coords(const OzGemmArgs& a, long t, int& bm, int& bn) {
-  if (a.lower) {  // t -> (bm >= bn), t = bm (bm + 1) / 2 + bn
-    long i = (long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-    while (i * (i + 1) / 2 > t) --i;
-    while ((i + 1) * (i + 2) / 2 <= t) ++i;
-    bm = (int)i;
-    bn = (int)(t - i * (i + 1) / 2);
+  if (a.lower) {
+    // column-block bn holds tile rows 2 bn .. tiles_m - 1 (rows of 128 meet
+    // columns of 256 at or below the diagonal)
+    int c = 0;
+    for (;; ++c) {
+      const long cnt = a.tiles_m - 2L * c;
+      if (t < cnt) break;
+      t -= cnt;
+    }
+    bn = c;
+    bm = 2 * c + (int)t;
     return;
   }
   // groups of kOzGroup tile rows, column-major inside a group
@@ -224,34 +243,42 @@ __device__ __forceinline__ void tile_coords(const OzGemmArgs& a, long t, int& bm
   bn = (int)(r / rows);
 }
 
+__device__ __forceinline__ void mbar_arrive_cta(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
 template <int STAGES>
-__global__ void __launch_bounds__(kOzThreads, 1)
+__global__ void __launch_bounds__(kPThreads, 1)
     oz_imma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                    const OzGemmArgs a) {
   extern __shared__ __align__(1024) uint8_t osm[];
   uint8_t* stages = osm + ((1024u - (smem_u32(osm) & 1023u)) & 1023u);
-  uint64_t* full = reinterpret_cast<uint64_t*>(stages + STAGES * kOzStageBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + STAGES * kPStage);
   uint64_t* empty = full + STAGES;
-  uint64_t* done = empty + STAGES;
+  uint64_t* tfull = empty + STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* done = tempty + 2;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int l = blockIdx.y;
-  int bm, bn;
-  tile_coords(a, blockIdx.x, bm, bn);
-  const long m0 = (long)bm * kOzBM, n0 = (long)bn * kOzBN;
-  const long nk = (a.K + kOzBK - 1) / kOzBK;
+  const long nk = (a.K + kPK - 1) / kPK;
+  const long total = a.tiles_per_mod * a.nmod;
 
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
     }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull + b, 1);
+      mbar_init(tempty + b, 128);
+    }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
                      smem_u32(tslot))
                  : "memory");
@@ -262,92 +289,126 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
 
-  bool ok = true;
   if (warp == 0) {
-    if (lane == 0) {  // TMA producer
-      for (long kb = 0; kb < nk; ++kb) {
-        const int s = (int)(kb % STAGES);
-        if (kb >= STAGES &&
-            !mbar_wait(empty + s, (uint32_t)((kb / STAGES - 1) & 1), a.err)) {
-          ok = false;
-          break;
+    if (lane == 0) {  // ---- TMA producer ----
+      long gk = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        const int l = (int)(t / a.tiles_per_mod);
+        int bm, bn;
+        tile_coords(a, t % a.tiles_per_mod, bm, bn);
+        for (long kb = 0; kb < nk; ++kb, ++gk) {
+          const int s = (int)(gk % STAGES);
+          if (gk >= STAGES &&
+              !mbar_wait(empty + s, (uint32_t)((gk / STAGES - 1) & 1), a.err)) {
+            ok = false;
+            break;
+          }
+          uint8_t* sa = stages + s * kPStage;
+          mbar_expect_tx(full + s, kPStage);
+          tma_load3(sa, &mapA, (int)(kb * kPK), bm * kPM, l, full + s);
+          tma_load3(sa + kPTileA, &mapB, (int)(kb * kPK), bn * kPN, l, full + s);
         }
-        uint8_t* sa = stages + s * kOzStageBytes;
-        mbar_expect_tx(full + s, kOzStageBytes);
-        tma_load3(sa, &mapA, (int)(kb * kOzBK), (int)m0, l, full + s);
-        tma_load3(sa + kOzTile, &mapB, (int)(kb * kOzBK), (int)n0, l, full + s);
       }
     }
-    __syncwarp();
   } else if (warp == 1) {
-    if (lane == 0) {  // MMA issuer
-      for (long kb = 0; kb < nk; ++kb) {
-        const int s = (int)(kb % STAGES);
-        if (!mbar_wait(full + s, (uint32_t)((kb / STAGES) & 1), a.err)) {
-          ok = false;
-          break;
-        }
+    if (lane == 0) {  // ---- MMA issuer ----
+      long gk = 0;
+      int i = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < total && ok; t += gridDim.x, ++i) {
+        const int b = i & 1;
+        if (i >= 2 && !mbar_wait(tempty + b, (uint32_t)(((i >> 1) - 1) & 1), a.err)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t sa = smem_u32(stages + s * kOzStageBytes);
-        const uint32_t sb = sa + kOzTile;
+        const uint32_t acc_tm = tmem + (uint32_t)(b * kPN);
+        for (long kb = 0; kb < nk; ++kb, ++gk) {
+          const int s = (int)(gk % STAGES);
+          if (!mbar_wait(full + s, (uint32_t)((gk / STAGES) & 1), a.err)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sa = smem_u32(stages + s * kPStage);
+          const uint32_t sb = sa + kPTileA;
 #pragma unroll
-        for (int ks = 0; ks < kOzBK / 32; ++ks) {
-          const uint32_t acc = (kb > 0 || ks > 0) ? 1u : 0u;
-          const uint64_t db = smem_desc_sw128(sb + ks * 32);
-          umma_i8(tmem, smem_desc_sw128(sa + ks * 32), db, acc);
-          umma_i8(tmem + kOzMmaN, smem_desc_sw128(sa + kOzTile / 2 + ks * 32), db, acc);
+          for (int ks = 0; ks < kPK / 32; ++ks)
+            umma_i8(acc_tm, smem_desc_sw128(sa + ks * 32), smem_desc_sw128(sb + ks * 32),
+                    (kb > 0 || ks > 0) ? 1u : 0u);
+          umma_commit(empty + s);
         }
-        umma_commit(empty + s);
+        if (ok) umma_commit(tfull + b);
       }
       umma_commit(done);  // fires when every MMA issued above has completed
+      mbar_wait(done, 0, a.err);
     }
-    __syncwarp();
-  }
-  const bool fin = mbar_wait(done, 0, a.err);
-  ok = __syncthreads_and(ok && fin);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok) {
-    // epilogue: warp w reads TMEM lanes 32w..32w+31 = tile rows 32w + lane
-    // (accumulator 0) and 128 + 32w + lane (accumulator 1)
-    const int p = a.p[l];
-    const unsigned magic = a.magic[l];
-    // |acc| <= K 2^14 <= 2^30 < p 2^23 (K <= 2^16, p >= 173): acc + off is in
-    // [0, 2^32) and congruent to acc mod p
-    const unsigned off = (unsigned)p << 23;
-    uint8_t* R = a.R + (long)l * a.plane;
+  } else {  // ---- epilogue: warps 2-5, TMEM lanes 32 (warp % 4) .. + 31 ----
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    int i = 0;
+    for (long t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      if (!mbar_wait(tfull + b, (uint32_t)((i >> 1) & 1), a.err)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int l = (int)(t / a.tiles_per_mod);
+      int bm, bn;
+      tile_coords(a, t % a.tiles_per_mod, bm, bn);
+      const int p = a.p[l];
+      const unsigned magic = a.magic[l];
+      // |acc| <= K 2^14 <= 2^30 < p 2^23 (K <= 2^16, p >= 193): acc + off is in
+      // [0, 2^32) and congruent to acc mod p
+      const unsigned off = (unsigned)p << 23;
+      uint8_t* R = a.R + (long)l * a.plane;
+      const long gm = (long)bm * kPM + row;
+      const long n0 = (long)bn * kPN;
+      // 64 columns per wait: four x16 loads in flight, then the reductions
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-      const long gm = m0 + h * 128 + warp * 32 + lane;
-#pragma unroll 1
-      for (int c0 = 0; c0 < kOzBN; c0 += 16) {
-        uint32_t v[16];
-        const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * kOzMmaN + c0);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-            "%10, %11, %12, %13, %14, %15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(addr));
+      for (int c0 = 0; c0 < kPN; c0 += 64) {
+        uint32_t v[64];
+        const uint32_t addr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kPN + c0);
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+              "%10, %11, %12, %13, %14, %15}, [%16];"
+              : "=r"(v[16 * h + 0]), "=r"(v[16 * h + 1]), "=r"(v[16 * h + 2]),
+                "=r"(v[16 * h + 3]), "=r"(v[16 * h + 4]), "=r"(v[16 * h + 5]),
+                "=r"(v[16 * h + 6]), "=r"(v[16 * h + 7]), "=r"(v[16 * h + 8]),
+                "=r"(v[16 * h + 9]), "=r"(v[16 * h + 10]), "=r"(v[16 * h + 11]),
+                "=r"(v[16 * h + 12]), "=r"(v[16 * h + 13]), "=r"(v[16 * h + 14]),
+                "=r"(v[16 * h + 15])
+              : "r"(addr + 16 * h));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (gm < a.M) {
+          uint8_t* dst = R + gm + (n0 + c0) * a.ldr;
+          const long left = a.N - (n0 + c0);
+          const unsigned ldr = (unsigned)a.ldr;  // a plane is < 2^32 bytes
+          if (left >= 64) {
+            unsigned o = 0;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const long gn = n0 + c0 + j;
-            if (gn < a.N) {
+            for (int j = 0; j < 64; ++j, o += ldr) {
               const unsigned x = v[j] + off;
               unsigned r = x - __umulhi(x, magic) * (unsigned)p;  // in [0, 2p)
-              if (r >= (unsigned)p) r -= (unsigned)p;
-              R[gm + gn * a.ldr] = (uint8_t)r;
+              r = (r >= (unsigned)p) ? r - (unsigned)p : r;
+              dst[o] = (uint8_t)r;
+            }
+          } else {
+            for (int j = 0; j < (int)left; ++j) {
+              const unsigned x = v[j] + off;
+              unsigned r = x - __umulhi(x, magic) * (unsigned)p;
+              r = (r >= (unsigned)p) ? r - (unsigned)p : r;
+              dst[(long)j * a.ldr] = (uint8_t)r;
             }
           }
         }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive_cta(tempty + b);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0)
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
@@ -383,21 +444,33 @@ __global__ void oz_quant_kernel(long rows, long K, const double* __restrict__ S,
     __syncthreads();
     const double scale = sscale;
     for (long k0 = 4 * (long)threadIdx.x; k0 < K; k0 += 4 * (long)blockDim.x) {
-      double v[4];
+      // the integers |v| <= 2^53 as 16-bit limbs d3 2^48 + d2 2^32 + d1 2^16 +
+      // d0 (d3 signed): v mod p = (d3 k48 + d2 k32 + d1 k16 + d0) mod p in
+      // 32-bit integers, reduced by a Barrett step
+      int d0[4], d1[4], d2[4], d3[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) v[q] = (k0 + q < K) ? rint(col[k0 + q] * scale) : 0.0;
+      for (int q = 0; q < 4; ++q) {
+        const long long t =
+            (k0 + q < K) ? (long long)rint(col[k0 + q] * scale) : 0LL;
+        d0[q] = (int)(t & 0xFFFF);
+        d1[q] = (int)((t >> 16) & 0xFFFF);
+        d2[q] = (int)((t >> 32) & 0xFFFF);
+        d3[q] = (int)(t >> 48);
+      }
       for (int li = 0; li < c.nmod; ++li) {
-        const double p = (double)c.p[li];
-        const int half = (c.p[li] + 1) >> 1;
+        const int p = c.p[li];
+        const unsigned magic = c.magic[li];
+        const int half = (p + 1) >> 1;
+        const int off = p << 17;  // > 32 * 255 = max |d3 k48|: keeps the sum positive
         char4 o;
         int8_t* ob = reinterpret_cast<int8_t*>(&o);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          double rr = fma(-floor(v[q] * c.invp[li]), p, v[q]);
-          if (rr < 0.0) rr += p;
-          if (rr >= p) rr -= p;
-          int ri = (int)rr;
-          if (ri >= half) ri -= c.p[li];
+          const unsigned x =
+              (unsigned)(d0[q] + off + d1[q] * c.k16[li] + d2[q] * c.k32[li] + d3[q] * c.k48[li]);
+          int ri = (int)(x - __umulhi(x, magic) * (unsigned)p);  // in [0, 2p)
+          if (ri >= p) ri -= p;
+          if (ri >= half) ri -= p;
           ob[q] = (int8_t)ri;
         }
         int8_t* dst = Q + (long)li * plane + r * ldq + k0;
@@ -444,19 +517,14 @@ __device__ __forceinline__ double limbs_value(const double (&x)[kOzLimbs]) {
   return fma(x[3], 0x1p120, fma(x[2], 0x1p80, fma(x[1], 0x1p40, x[0])));
 }
 
-// The integer in (-Mod/2, Mod/2) with residues R[l * plane + idx] as a double:
-// S = sum_l r_l w_l (limb sums exact), X = S - q Mod with q from a rounded
+// The integer in (-Mod/2, Mod/2) with given residues, as a double: from the
+// limb sums S = sum_l r_l w_l (exact), X = S - q Mod with q from a rounded
 // quotient, then the representative nearest zero (the product's bound keeps
 // the true value within Mod/4, far from the decision points), then the
 // magnitude's limbs summed from the top limb down (each step one rounding).
-__device__ __forceinline__ double crt_value(const uint8_t* __restrict__ R, long plane, long idx,
-                                            const OzConsts& c) {
-  double x[kOzLimbs] = {0.0, 0.0, 0.0, 0.0};
-  for (int li = 0; li < c.nmod; ++li) {
-    const double r = (double)R[li * plane + idx];
-#pragma unroll
-    for (int i = 0; i < kOzLimbs; ++i) x[i] = fma(r, c.wl[i][li], x[i]);
-  }
+// X = sum_l r_l w_l (limb sums, exact) -> the representative in
+// (-Mod/2, Mod/2) as a double
+__device__ __forceinline__ double crt_finish(double (&x)[kOzLimbs], const OzConsts& c) {
   const double q = floor(limbs_value(x) * c.invM);
 #pragma unroll
   for (int i = 0; i < kOzLimbs; ++i) x[i] = fma(-q, c.ml[i], x[i]);
@@ -480,35 +548,85 @@ __device__ __forceinline__ double crt_value(const uint8_t* __restrict__ R, long 
 
 // D(m, n) = alpha 2^-(ea_m + eb_n) crt(m, n) + beta C(m, n) + diag [m == n].
 // lower: only m >= n is rebuilt and D(n, m) receives the same value (a
-// symmetric product).  32 x 32 tiles (threads 32 x 8); the mirrored writes go
+// symmetric product).  Tiles of 128 rows x 32 columns, 256 threads: thread
+// (g = t % 32, c = t / 32) rebuilds rows 4g..4g+3 of columns c, c+8, c+16,
+// c+24 (one 4-byte load per modulus and column); the mirrored writes go
 // through shared memory so that both stores are coalesced.
-__global__ void oz_crt_kernel(long M, long N, const uint8_t* __restrict__ R, long ldr, long plane,
-                              const int* __restrict__ ea, const int* __restrict__ eb, double alpha,
-                              double beta, const double* C, long ldc, double diag, double* D,
-                              long ldd, int lower, const OzConsts c) {
-  __shared__ double t[32][33];
-  const long i0 = (long)blockIdx.x * 32, j0 = (long)blockIdx.y * 32;
-  if (lower && j0 > i0) return;
-  const long i = i0 + threadIdx.x;
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const long j = j0 + r;
-    double out = 0.0;
-    const bool in = i < M && j < N && (!lower || i >= j);
-    if (in) {
-      const double v = crt_value(R, plane, i + j * ldr, c);
-      out = alpha * ldexp(v, -(ea[i] + eb[j]));
-      if (beta != 0.0) out = fma(beta, C[i + j * ldc], out);
-      if (i == j) out += diag;
-      D[i + j * ldd] = out;
+constexpr int kCrtRows = 128, kCrtCols = 32;
+template <int NL>
+__global__ void __launch_bounds__(256)
+    oz_crt_kernel(long M, long N, const uint8_t* __restrict__ R, long ldr, long plane,
+                  const int* __restrict__ ea, const int* __restrict__ eb, double alpha,
+                  double beta, const double* C, long ldc, double diag, double* D, long ldd,
+                  int lower, const OzConsts c) {
+  __shared__ double t[kCrtCols][kCrtRows + 1];
+  const long i0 = (long)blockIdx.x * kCrtRows, j0 = (long)blockIdx.y * kCrtCols;
+  if (lower && j0 >= i0 + kCrtRows) return;  // the tile lies above the diagonal
+  const int g = threadIdx.x & 31, cc = threadIdx.x >> 5;
+  const long ib = i0 + 4 * g;
+  const bool full4 = ib + 3 < M && (ldr & 3) == 0;
+#pragma unroll 1
+  for (int q = 0; q < 4; ++q) {
+    const int cl = cc + 8 * q;
+    const long j = j0 + cl;
+    double out[4] = {0.0, 0.0, 0.0, 0.0};
+    if (j < N && (!lower || ib + 3 >= j)) {
+      // residues of the 4 rows, modulus by modulus
+      double x[4][kOzLimbs];
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+#pragma unroll
+        for (int i = 0; i < kOzLimbs; ++i) x[e][i] = 0.0;
+      const uint8_t* base = R + ib + j * ldr;
+      // all residue words first (loads in flight together), then the sums
+      uint32_t w4[kOzMaxMod];
+#pragma unroll
+      for (int li = 0; li < kOzMaxMod; ++li) {
+        w4[li] = 0;
+        if (li < c.nmod) {
+          if (full4) {
+            w4[li] = __ldg(reinterpret_cast<const uint32_t*>(base + li * plane));
+          } else {
+            for (int e = 0; e < 4; ++e)
+              if (ib + e < M) w4[li] |= (uint32_t)base[li * plane + e] << (8 * e);
+          }
+        }
+      }
+#pragma unroll
+      for (int li = 0; li < kOzMaxMod; ++li) {
+        if (li < c.nmod) {
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            // byte -> double without a conversion instruction: 2^52 + r as bits
+            const double r = __hiloint2double(0x43300000, (int)((w4[li] >> (8 * e)) & 0xFFu)) -
+                             4503599627370496.0;
+#pragma unroll
+            for (int i = 0; i < NL; ++i) x[e][i] = fma(r, c.wl[i][li], x[e][i]);
+          }
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const long i = ib + e;
+        if (i < M && (!lower || i >= j)) {
+          const double v = crt_finish(x[e], c);
+          double o = alpha * ldexp(v, -(ea[i] + eb[j]));
+          if (beta != 0.0) o = fma(beta, C[i + j * ldc], o);
+          if (i == j) o += diag;
+          D[i + j * ldd] = o;
+          out[e] = o;
+        }
+      }
     }
-    t[r][threadIdx.x] = out;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) t[cl][4 * g + e] = out[e];
   }
   if (!lower) return;
   __syncthreads();
-  // mirror: D(j, i) for i > j, rows j0 + tx
-  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-    const long ii = i0 + r, jj = j0 + threadIdx.x;  // element (ii, jj) computed above, ii >= jj
-    if (ii < M && jj < N && ii > jj) D[jj + ii * ldd] = t[threadIdx.x][r];
+  // mirror: D(j, i) = D(i, j) for i > j; a warp writes 32 consecutive j of one i
+  for (int r = threadIdx.x >> 5; r < kCrtRows; r += 8) {
+    const long i = i0 + r, j = j0 + (threadIdx.x & 31);
+    if (i < M && j < N && i > j) D[j + i * ldd] = t[threadIdx.x & 31][r];
   }
 }
 
@@ -543,12 +661,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // planes of int8 rows (K bytes used of ld), `rows` rows per plane, nmod planes
 int make_plane_map(CUtensorMap* map, const int8_t* base, long rows, long K, long ld, long plane,
-                   int nmod) {
+                   int nmod, int box_rows) {
   auto enc = encode_fn();
   if (!enc) return EVD_ERR_CUDA;
   cuuint64_t dims[3] = {(cuuint64_t)K, (cuuint64_t)rows, (cuuint64_t)nmod};
   cuuint64_t strides[2] = {(cuuint64_t)ld, (cuuint64_t)plane};
-  cuuint32_t box[3] = {(cuuint32_t)kOzBK, (cuuint32_t)kOzBM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)kPK, (cuuint32_t)box_rows, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)base, dims, strides, box, es,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -619,14 +737,15 @@ int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t*
   if (K <= 0 || K > kOzMaxK) return EVD_ERR_INVALID_ARG;  // INT32 accumulation bound
   const long ldq = oz_ld(K);
   CUtensorMap ma, mb;
-  EVD_TRY(make_plane_map(&ma, QA, M, K, ldq, M * ldq, nmod));
-  EVD_TRY(make_plane_map(&mb, QB, N, K, ldq, N * ldq, nmod));
+  EVD_TRY(make_plane_map(&ma, QA, M, K, ldq, M * ldq, nmod, kPM));
+  EVD_TRY(make_plane_map(&mb, QB, N, K, ldq, N * ldq, nmod, kPN));
   const OzConsts c = make_consts(nmod, K);
   OzGemmArgs a{};
   a.M = M; a.N = N; a.K = K;
-  a.tiles_m = ceil_div_i(M, kOzBM);
-  a.tiles_n = ceil_div_i(N, kOzBN);
+  a.tiles_m = ceil_div_i(M, kPM);
+  a.tiles_n = ceil_div_i(N, kPN);
   a.lower = lower ? 1 : 0;
+  a.nmod = nmod;
   a.R = Rz;
   a.ldr = (M + 15) / 16 * 16;
   a.plane = a.ldr * N;
@@ -636,14 +755,21 @@ int oz_imma(long M, long N, long K, const int8_t* QA, const int8_t* QB, uint8_t*
   }
   a.err = oz_err_word();
   if (!a.err) return EVD_ERR_CUDA;
-  const long tiles = lower ? (long)a.tiles_m * (a.tiles_m + 1) / 2 : (long)a.tiles_m * a.tiles_n;
-  if (tiles >= (1L << 31) || nmod > 65535) return EVD_ERR_INVALID_ARG;
+  long tiles = 0;
+  if (lower) {
+    for (long bn = 0; 2 * bn < a.tiles_m; ++bn) tiles += a.tiles_m - 2 * bn;
+  } else {
+    tiles = (long)a.tiles_m * a.tiles_n;
+  }
+  a.tiles_per_mod = tiles;
+  const long total = tiles * nmod;
+  const int grid = (int)std::min<long>(total, device_sm_count());
   if (lean) {
     EVD_TRY(smem_attr_once((const void*)oz_imma_kernel<2>, oz_smem(2)));
-    oz_imma_kernel<2><<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, oz_smem(2), st>>>(ma, mb, a);
+    oz_imma_kernel<2><<<grid, kPThreads, oz_smem(2), st>>>(ma, mb, a);
   } else {
-    EVD_TRY(smem_attr_once((const void*)oz_imma_kernel<3>, oz_smem(3)));
-    oz_imma_kernel<3><<<dim3((unsigned)tiles, (unsigned)nmod), kOzThreads, oz_smem(3), st>>>(ma, mb, a);
+    EVD_TRY(smem_attr_once((const void*)oz_imma_kernel<4>, oz_smem(4)));
+    oz_imma_kernel<4><<<grid, kPThreads, oz_smem(4), st>>>(ma, mb, a);
   }
   EVD_LAUNCHED();
   return EVD_SUCCESS;
@@ -655,8 +781,13 @@ int oz_crt(long M, long N, long K, const uint8_t* Rz, const int* ea, const int* 
   if (M <= 0 || N <= 0) return EVD_SUCCESS;
   const OzConsts c = make_consts(nmod, K);
   const long ldr = (M + 15) / 16 * 16;
-  oz_crt_kernel<<<dim3(ceil_div_i(M, 32), ceil_div_i(N, 32)), dim3(32, 8), 0, st>>>(
-      M, N, Rz, ldr, ldr * N, ea, eb, alpha, beta, C, ldc, diag, D, ldd, lower ? 1 : 0, c);
+  const dim3 grid(ceil_div_i(M, kCrtRows), ceil_div_i(N, kCrtCols));
+  if (c.nlimb == 3)
+    oz_crt_kernel<3><<<grid, 256, 0, st>>>(M, N, Rz, ldr, ldr * N, ea, eb, alpha, beta, C, ldc,
+                                           diag, D, ldd, lower ? 1 : 0, c);
+  else
+    oz_crt_kernel<4><<<grid, 256, 0, st>>>(M, N, Rz, ldr, ldr * N, ea, eb, alpha, beta, C, ldc,
+                                           diag, D, ldd, lower ? 1 : 0, c);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }

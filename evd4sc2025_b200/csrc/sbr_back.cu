@@ -75,19 +75,16 @@ long sbr_back_ws_doubles(long n, long b, long nk) {
   return std::max(n * nk / 2, nk * n) + 64;
 }
 
-// Emulated-product workspace of sbr_apply_slabs (bytes): the larger of its
-// two products' (T = Y_s^T X with K = rows, X -= W_s T with K = nk).
-long sbr_apply_oz_bytes(long n, long nk, long ncols, int nmod) {
-  return std::max(oz_layout(nk, ncols, n, nmod, false).bytes,
-                  oz_layout(n, ncols, nk, nmod, true).bytes);
+// Emulated-product workspace of sbr_form_q1 (bytes): the larger of its two
+// products' (T = Y_s^T M with K = rows, M -= W_s T with K = nk).
+long sbr_form_oz_bytes(long n, long nk, int nmod) {
+  return std::max(oz_layout(nk, n, n, nmod, false).bytes, oz_layout(n, n, nk, nmod, true).bytes);
 }
 
-// X <- Q1 X using slab-merged W (call wy_merge_slabs first).  oz != nullptr:
-// both products of every slab are emulated FP64 products on the integer
-// tensor cores.
+// X <- Q1 X using slab-merged W (call wy_merge_slabs first).
 int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const double* dY,
                     long ldY, double* X, long ldX, long ncols, double* work, size_t work_n,
-                    cudaStream_t st, const OzWork* oz) {
+                    cudaStream_t st) {
   const long npcols = ((n - 1) / b) * b;  // panel columns (stage 1 leaves the last b-block)
   if (npcols <= 0 || ncols <= 0) return EVD_SUCCESS;
   const long nslabs = (npcols + nk - 1) / nk;
@@ -99,13 +96,6 @@ int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const d
     if (m <= 0 || w <= 0) continue;
     // T = Y_s^T X[r0:, :]  (w x ncols), then X[r0:, :] -= W_s T
     if ((size_t)(w * ncols) > work_n) return EVD_ERR_WORKSPACE;
-    if (oz) {
-      EVD_TRY(oz_gemm('t', 'n', w, ncols, m, 1.0, dY + r0 + c0 * ldY, ldY, X + r0, ldX, 0.0,
-                      nullptr, w, 0.0, work, w, oz->nmod, false, oz->ws, oz->bytes, st));
-      EVD_TRY(oz_gemm('n', 'n', m, ncols, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, X + r0,
-                      ldX, 0.0, X + r0, ldX, oz->nmod, false, oz->ws, oz->bytes, st));
-      continue;
-    }
     EVD_TRY(dgemm('t', 'n', w, ncols, m, 1.0, dY + r0 + c0 * ldY, ldY, X + r0, ldX, 0.0, work, w,
                   st));
     EVD_TRY(dgemm('n', 'n', m, ncols, w, -1.0, dW + r0 + c0 * ldW, ldW, work, w, 1.0, X + r0,
@@ -172,7 +162,7 @@ extern "C" int evd_sbr_back(long n, long b, long nk, double* dW, long ldW, const
   const long npcols = ((n - 1) / b) * b;
   EVD_TRY(evd::wy_merge_slabs(n, b, nk, npcols, dW, ldW, dY, ldY, work, stream));
   return evd::sbr_apply_slabs(n, b, nk, dW, ldW, dY, ldY, X, ldX, ncols, work, (size_t)lwork,
-                              stream, nullptr);
+                              stream);
 }
 
 extern "C" int evd_wy_from_slide(long M, long N, long slideWidth, double* dW, long ldW,

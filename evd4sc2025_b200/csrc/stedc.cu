@@ -32,6 +32,7 @@
 
 #include "common.cuh"
 #include "gemm_f64.cuh"
+#include "ozaki.cuh"
 
 namespace evd {
 
@@ -827,8 +828,13 @@ __global__ void finish_kernel(long n, long np, const double* dw, const double* Z
 long stedc_ws_doubles(long n) { return n <= 1 ? 8 : make_plan(n).total_d; }
 long stedc_ws_ints(long n) { return n <= 1 ? 8 : make_plan(n).total_i; }
 
+// oz != nullptr: merges whose products exceed kOzMergeMin multiply-adds run
+// them as emulated FP64 products on the integer tensor cores (one per merge),
+// the smaller ones stay on the batched DMMA GEMM.
+constexpr double kOzMergeMin = 64.0 * 1024 * 1024 * 1024;
+
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
-          long liwork, cudaStream_t st) {
+          long liwork, cudaStream_t st, const OzWork* oz) {
   if (n < 0 || ldz < std::max(1L, n)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (!d || !Z || !work || !iwork || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;
@@ -950,15 +956,32 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
       EVD_LAUNCHED();
       // Zn[0:n1, 0:Kmax] = Qt Ut ; Zn[n1:N, 0:Kmax] = Qb Ub   (batched over merges)
       const long sZ = (long)a.N * a.N;
+      const bool emul = oz && (double)a.n1 * Kmax * std::max(K12, K23) >= kOzMergeMin;
       if (K12 > 0) {
-        EVD_TRY(dgemm_batched('n', 'n', a.n1, Kmax, K12, 1.0, a.Qt, a.n1, (long)a.n1 * a.K12max,
-                              a.Ut, a.K12max, (long)a.K12max * Kmax, 0.0, a.Zn, a.N, sZ, a.nm,
-                              st));
+        if (emul) {
+          for (int m = 0; m < a.nm; ++m)
+            EVD_TRY(oz_gemm('n', 'n', a.n1, Kmax, K12, 1.0, a.Qt + (long)m * a.n1 * a.K12max,
+                            a.n1, a.Ut + (long)m * a.K12max * Kmax, a.K12max, 0.0, nullptr, a.N,
+                            0.0, a.Zn + (long)m * sZ, a.N, oz->nmod, false, oz->ws, oz->bytes,
+                            st));
+        } else {
+          EVD_TRY(dgemm_batched('n', 'n', a.n1, Kmax, K12, 1.0, a.Qt, a.n1,
+                                (long)a.n1 * a.K12max, a.Ut, a.K12max, (long)a.K12max * Kmax,
+                                0.0, a.Zn, a.N, sZ, a.nm, st));
+        }
       }
       if (K23 > 0) {
-        EVD_TRY(dgemm_batched('n', 'n', a.n2, Kmax, K23, 1.0, a.Qb, a.n2, (long)a.n2 * a.K23max,
-                              a.Ub, a.K23max, (long)a.K23max * Kmax, 0.0, a.Zn + a.n1, a.N, sZ,
-                              a.nm, st));
+        if (emul) {
+          for (int m = 0; m < a.nm; ++m)
+            EVD_TRY(oz_gemm('n', 'n', a.n2, Kmax, K23, 1.0, a.Qb + (long)m * a.n2 * a.K23max,
+                            a.n2, a.Ub + (long)m * a.K23max * Kmax, a.K23max, 0.0, nullptr, a.N,
+                            0.0, a.Zn + a.n1 + (long)m * sZ, a.N, oz->nmod, false, oz->ws,
+                            oz->bytes, st));
+        } else {
+          EVD_TRY(dgemm_batched('n', 'n', a.n2, Kmax, K23, 1.0, a.Qb, a.n2,
+                                (long)a.n2 * a.K23max, a.Ub, a.K23max, (long)a.K23max * Kmax,
+                                0.0, a.Zn + a.n1, a.N, sZ, a.nm, st));
+        }
       }
       if (K12 == 0 || K23 == 0) {
         // the missing half of the root columns is zero
@@ -991,5 +1014,5 @@ extern "C" long evd_stedc_iwork_size(long n) { return evd::stedc_ws_ints(n < 0 ?
 
 extern "C" int evd_stedc(long n, double* d, double* e, double* Z, long ldz, double* work,
                          long lwork, int* iwork, long liwork, cudaStream_t stream) {
-  return evd::stedc(n, d, e, Z, ldz, work, lwork, iwork, liwork, stream);
+  return evd::stedc(n, d, e, Z, ldz, work, lwork, iwork, liwork, stream, nullptr);
 }

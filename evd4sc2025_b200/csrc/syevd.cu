@@ -38,7 +38,7 @@ long stedc_ws_doubles(long n);
 int stebz(long n, const double* d, const double* e, double* w, double* work, cudaStream_t st);
 long stedc_ws_ints(long n);
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
-          long liwork, cudaStream_t st);
+          long liwork, cudaStream_t st, const OzWork* oz);
 long q2_tbuf_doubles(long n);
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
              double* tbuf, cudaStream_t st);
@@ -47,8 +47,8 @@ int wy_merge_slabs(long n, long b, long nk, long ncolsWY, double* dW, long ldW, 
                    long ldY, double* work, cudaStream_t st);
 int sbr_apply_slabs(long n, long b, long nk, const double* dW, long ldW, const double* dY,
                     long ldY, double* X, long ldX, long ncols, double* work, size_t work_n,
-                    cudaStream_t st, const OzWork* oz);
-long sbr_apply_oz_bytes(long n, long nk, long ncols, int nmod);
+                    cudaStream_t st);
+long sbr_form_oz_bytes(long n, long nk, int nmod);
 int sbr_form_q1(long n, long b, long nk, const double* dW, long ldW, const double* dY, long ldY,
                 double* M, long ldM, double* work, size_t work_n, cudaStream_t st,
                 const OzWork* oz, bool lean);
@@ -75,8 +75,10 @@ struct MixedOpts {
 // integer workspace of the mixed solve for order n (padded)
 long mixed_oz_bytes(long n, long nb, int nmod, int refine_iters) {
   long need = std::max(oz_syr2k_ws_bytes(std::max(n - nb, 1L), nb, nmod),
-                       sbr_apply_oz_bytes(n, nb, n, nmod));
-  need = std::max(need, oz_layout(n, n, n, nmod, false).bytes);  // X = Q Z
+                       sbr_form_oz_bytes(n, nb, nmod));
+  // X = Q Z, and the divide and conquer's largest merge products (their
+  // left operand is transposed first)
+  need = std::max(need, oz_layout(n, n, n, nmod, true).bytes);
   if (refine_iters > 0) need = std::max(need, refine_oz_int_bytes(n, kOzFp64Mod));
   return need + 512;
 }
@@ -164,7 +166,7 @@ struct NvtxRange {
 // returned so the caller can enqueue more work before the one host read.
 static int syevd_core(long n, long b, long nb, const double* A, long lda, double* w, double* X,
                       long ldX, void* work, long lwork_bytes, int timed, cudaStream_t st,
-                      const int** err_out = nullptr, const MixedOpts* mx = nullptr) {
+                      const int** err_out = nullptr) {
   if (n <= 0 || b != 32 || nb <= 0 || nb % b != 0 || n % nb != 0) return EVD_ERR_INVALID_ARG;
   long q = nb / b;
   if (q & (q - 1)) return EVD_ERR_INVALID_ARG;  // slab merge needs nb = b * 2^k
@@ -180,13 +182,7 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
   int* ich = ibase + L.oIchase;
   int* ist = ibase + L.oIstedc;
 
-  OzWork ozw{0, nullptr, 0};
-  const OzWork* oz = nullptr;
-  if (mx && mx->nmod > 0) {
-    ozw = OzWork{mx->nmod, mx->oz, mx->oz_bytes};
-    oz = &ozw;
-  }
-  cudaEvent_t ev[7];
+  cudaEvent_t ev[6];
   if (timed) {
     for (auto& x : ev) EVD_CUDA_TRY(cudaEventCreate(&x));
     EVD_CUDA_TRY(cudaEventRecord(ev[0], st));
@@ -198,7 +194,7 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
     EVD_CUDA_TRY(cudaMemsetAsync(W, 0, sizeof(double) * n * n, st));
     EVD_CUDA_TRY(cudaMemsetAsync(Y, 0, sizeof(double) * n * n, st));
     EVD_TRY(sy2sb(n, n, b, nb, OA, n, dA, n, W, n, Y, n, Z, n, R, n, S,
-                  (long)sy2sb_ws_doubles(n, b, nb), st, oz));
+                  (long)sy2sb_ws_doubles(n, b, nb), st, nullptr));
   }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[1], st));
   {  // ---- stage 2: band -> tridiagonal ----
@@ -211,7 +207,8 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
   {  // ---- tridiagonal D&C (eigenvectors straight into X) ----
     NvtxRange r("evd_b200 tridiagonal divide and conquer");
     EVD_TRY(
-        stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
+        stedc(n, d, e, X, ldX, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st,
+              nullptr));
   }
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[3], st));
   {  // ---- back transformations ----
@@ -227,29 +224,18 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
     const long npcols = ((n - 1) / b) * b;
     EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, st));
     EVD_TRY(sbr_apply_slabs(n, b, nb, W, n, Y, n, X, ldX, n, SB,
-                            (size_t)sbr_back_ws_doubles(n, b, nb), st, oz));
+                            (size_t)sbr_back_ws_doubles(n, b, nb), st));
   }
   EVD_CUDA_TRY(cudaMemcpyAsync(w, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[5], st));
-  if (mx && mx->refine_iters > 0) {
-    // Ogita-Aishima on the result; its FP64 buffers reuse OA, dA, W and Y
-    // (contiguous, 4 n^2 doubles, dead after the back transformations)
-    NvtxRange r("evd_b200 eigenpair refinement");
-    if ((size_t)refine_ws_doubles(n) > L.oY + (size_t)n * n) return EVD_ERR_WORKSPACE;
-    EVD_TRY(refine_syev_oz_split(n, A, lda, w, X, ldX, mx->refine_iters, kOzFp64Mod,
-                                 mx->moduli_update, OA, mx->oz, st));
-  }
   if (timed) {
-    EVD_CUDA_TRY(cudaEventRecord(ev[6], st));
-    EVD_CUDA_TRY(cudaEventSynchronize(ev[6]));
+    EVD_CUDA_TRY(cudaEventRecord(ev[5], st));
+    EVD_CUDA_TRY(cudaEventSynchronize(ev[5]));
     float ms;
     for (int i = 0; i < 5; ++i) {
       EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
       g_timings[i] = ms;
     }
-    EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[5], ev[6]));
-    g_refine_ms = ms;
-    EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[6]));
+    EVD_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[5]));
     g_timings[5] = ms;
     for (auto& x : ev) cudaEventDestroy(x);
   }
@@ -342,7 +328,8 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
   EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[3], 0));
   {
     NvtxRange r("evd_b200 tridiagonal divide and conquer");
-    EVD_TRY(stedc(n, d, e, W, n, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st));
+    EVD_TRY(stedc(n, d, e, W, n, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st,
+                  &oz));
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[6], st));
   EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[5], 0));
