@@ -466,6 +466,212 @@ __global__ void __launch_bounds__(kQThreads, 2)
   }
 }
 
+// ---- 8-column warps (m8n8k4), precomputed -V fragments ----
+// The same strips, blocks, group order and staged fragments as q2_mma_kernel
+// (PRE), with a warp owning 8 columns: the window tile (8 columns x 8 rows)
+// is the m8n8k4 accumulator (lane (g, t): column g, rows 2t and 2t+1), which
+// is the A operand of the W product for the rows {0, 2, 4, 6} (x[i][0]) and
+// {1, 3, 5, 7} (x[i][1]) with the B operand read from the same staged
+// reflector segments; W (column g, reflectors 2t, 2t+1) is in turn the A
+// operand of the update for the even and odd reflectors against the -V
+// fragments.  The window takes 68 registers instead of 136, so twice as many
+// warps share each sub-partition's tensor pipe (the kernel above is bound by
+// its dependent DMMA chains with two warps per sub-partition).
+constexpr int kQ8Cols = 8;
+
+__device__ __forceinline__ void w_part8(const double (&x)[kTiles][2], const double* ys, int offW,
+                                        int J, int i0, int i1, double (&wa)[2],
+                                        double (&wb)[2]) {
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    if (i < i0 || i >= i1) continue;
+    const int ti = 4 * J + i;
+    const double b0 = ys[offW + J * kSeg + 8 * i];
+    const double b1 = ys[offW + J * kSeg + 8 * i + 1];
+    if (i & 1) {
+      mma8(wb, x[ti][0], b0);
+      mma8(wb, x[ti][1], b1);
+    } else {
+      mma8(wa, x[ti][0], b0);
+      mma8(wa, x[ti][1], b1);
+    }
+  }
+}
+
+template <bool FWD>
+__device__ __forceinline__ void apply_block8(double (&x)[kTiles][2], const double* ys,
+                                             const double* ts, int lane, int offW) {
+  double wa[2] = {0.0, 0.0}, wb[2] = {0.0, 0.0};
+  w_part8(x, ys, offW, FWD ? kGroups - 1 : 0, 0, 5, wa, wb);
+#pragma unroll
+  for (int s = 0; s < kGroups; ++s) {
+    const int J = FWD ? kGroups - 1 - s : s;
+    const int JN = FWD ? J - 1 : J + 1;
+    const double wt0 = wa[0] + wb[0], wt1 = wa[1] + wb[1];
+    double na[2] = {0.0, 0.0}, nb[2] = {0.0, 0.0};
+    if (s + 1 < kGroups) w_part8(x, ys, offW, JN, FWD ? 0 : 1, FWD ? 4 : 5, na, nb);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const int i = FWD ? k : 4 - k;  // shared tile first
+      const int ti = 4 * J + i;
+      const double2 vf =
+          *reinterpret_cast<const double2*>(ts + J * kVGroup + (i * 32 + lane) * 2);
+      mma8(x[ti], wt0, vf.x);
+      mma8(x[ti], wt1, vf.y);
+    }
+    if (s + 1 < kGroups) {
+      w_part8(x, ys, offW, JN, FWD ? 4 : 0, FWD ? 5 : 1, na, nb);
+      wa[0] = na[0];
+      wa[1] = na[1];
+      wb[0] = nb[0];
+      wb[1] = nb[1];
+    }
+  }
+}
+
+__device__ __forceinline__ void load_tile8(double (&v)[2], const double* cg, bool ok, long row0,
+                                           int t2, int n) {
+  const long r = row0 + t2;
+  v[0] = (ok && r >= 0 && r < n) ? cg[r] : 0.0;
+  v[1] = (ok && r + 1 >= 0 && r + 1 < n) ? cg[r + 1] : 0.0;
+}
+__device__ __forceinline__ void store_tile8(const double (&v)[2], double* cg, bool ok, long row0,
+                                            int t2, int n) {
+  const long r = row0 + t2;
+  if (ok && r >= 0 && r < n) cg[r] = v[0];
+  if (ok && r + 1 >= 0 && r + 1 < n) cg[r + 1] = v[1];
+}
+
+template <bool FWD, int NW>
+__global__ void __launch_bounds__(NW * 32, 2)
+    q2_mma8_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
+                   const double* __restrict__ Tg, double* __restrict__ X, long ldX) {
+  extern __shared__ __align__(16) double smem[];
+  double* Ys = smem;                 // kNYBuf x kYBuf
+  double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kVBuf (-V fragments)
+  const int nthr = NW * 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  for (int e = threadIdx.x; e < kNYBuf * kYBuf; e += nthr) Ys[e] = 0.0;
+  const int offW = seg_off(g, 0) + 2 * t - g;  // Y[8i+2t(+1)][g]
+  const int c0 = blockIdx.x * (NW * kQ8Cols) + warp * kQ8Cols;
+  const bool okg = c0 + g < ncols;
+  double* cg = X + (long)(okg ? c0 + g : 0) * ldX;
+  const int t2 = 2 * t;
+
+  double x[kTiles][2];
+  const int nstrips = (n - 2 + kStrip - 1) / kStrip;
+  const int B0 = (n - 2 + 7) / 8;
+  auto stage_y = [&](double* ys, long R, int H, int bb) {
+    for (int e = threadIdx.x; e < 8 * kStrip; e += nthr) {
+      const int p = e / kStrip, i = e % kStrip;
+      const int h = 8 * bb + p;
+      const long row = R + h + 1 + i;
+      const bool valid = (h < H) && (row < n);
+      const double* src = valid ? (U + row + (long)h * ldU) : U;
+      cp_async8_zfill(ys + seg_off(p, i >> 5) + (i & 31), src, valid);
+    }
+  };
+  auto stage_t = [&](double* dst, int sidx, int bb) {
+    const double* src = Tg + tblock(sidx, bb, B0) * kVBuf;
+    for (int e = threadIdx.x; e < kVBuf / 2; e += nthr) cp_async16(dst + 2 * e, src + 2 * e);
+  };
+  for (int si = 0; si < nstrips; ++si) {
+    const int sidx = FWD ? (nstrips - 1 - si) : si;
+    const long R = (long)sidx * kStrip;
+    const int H = n - 2 - (int)R;
+    const int nblk = (H + 7) / 8;
+    auto bb_of = [&](int it) { return FWD ? it : (nblk - 1 - it); };
+
+    __syncthreads();
+    {
+      const long base = R + 8L * bb_of(0) + 1;
+#pragma unroll
+      for (int i = 0; i < kTiles; ++i) load_tile8(x[i], cg, okg, base + 8 * i, t2, n);
+    }
+    stage_y(Ys, R, H, bb_of(0));
+    stage_t(Ts, sidx, bb_of(0));
+    cp_commit();
+    if (nblk > 1) {
+      stage_y(Ys + kYBuf, R, H, bb_of(1));
+      stage_t(Ts + kVBuf, sidx, bb_of(1));
+    }
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();
+
+#pragma unroll 1
+    for (int it = 0; it < nblk; ++it) {
+      const int bb = bb_of(it);
+      const long base = R + 8L * bb + 1;
+      cp_wait<0>();
+      __syncthreads();
+      if (it + 2 < nblk) {
+        stage_y(Ys + ((it + 2) % 3) * kYBuf, R, H, bb_of(it + 2));
+        stage_t(Ts + ((it + 2) % 3) * kVBuf, sidx, bb_of(it + 2));
+      }
+      cp_commit();
+      double inc[2];
+      load_tile8(inc, cg, okg, FWD ? (base + 8 * kTiles) : (base - 8), t2, n);
+      apply_block8<FWD>(x, Ys + (it % 3) * kYBuf, Ts + (it % 3) * kVBuf, lane, offW);
+      if (FWD) {
+        store_tile8(x[0], cg, okg, base, t2, n);
+#pragma unroll
+        for (int i = 0; i + 1 < kTiles; ++i) {
+          x[i][0] = x[i + 1][0];
+          x[i][1] = x[i + 1][1];
+        }
+        x[kTiles - 1][0] = inc[0];
+        x[kTiles - 1][1] = inc[1];
+      } else {
+        store_tile8(x[kTiles - 1], cg, okg, base + 8 * (kTiles - 1), t2, n);
+#pragma unroll
+        for (int i = kTiles - 1; i > 0; --i) {
+          x[i][0] = x[i - 1][0];
+          x[i][1] = x[i - 1][1];
+        }
+        x[0][0] = inc[0];
+        x[0][1] = inc[1];
+      }
+    }
+    {
+      const long base = FWD ? (R + 8L * nblk + 1) : (R - 7);
+#pragma unroll
+      for (int i = 0; i < kTiles; ++i) store_tile8(x[i], cg, okg, base + 8 * i, t2, n);
+    }
+  }
+}
+
+constexpr size_t kQ8Smem = (size_t)(kNYBuf * kYBuf + kNYBuf * kVBuf) * sizeof(double);
+
+template <bool FWD, int NW>
+int launch_q2_8(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
+                long ldX, cudaStream_t st) {
+  EVD_TRY(smem_attr_once((const void*)q2_mma8_kernel<FWD, NW>, (int)kQ8Smem));
+  const int grid = ceil_div_i((int)ncols, NW * kQ8Cols);
+  q2_mma8_kernel<FWD, NW><<<grid, NW * 32, kQ8Smem, st>>>((int)n, (int)ncols, U, ldU, Tg, X, ldX);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+template <bool FWD, bool PRE>
+int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
+              long ldX, cudaStream_t st);
+
+// With fewer 64-column CTAs than SMs (ncols < 64 x SMs: n <= 8192 on B200)
+// the 16-column kernel leaves SMs idle; the 8-column kernel (4 warps, 32
+// columns per CTA) doubles the warps (n = 4096: 19.8 -> 14.0 ms).  Above that
+// the 16-column kernel is faster (n = 16384: 436 ms against 461 ms with
+// 8-column warps, whose m8n8k4 operands double the shared-memory reads per
+// flop).
+template <bool FWD>
+int launch_q2_pre(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
+                  long ldX, cudaStream_t st) {
+  if (ncols >= 64L * device_sm_count())
+    return launch_q2<FWD, true>(n, ncols, U, ldU, Tg, X, ldX, st);
+  return launch_q2_8<FWD, 4>(n, ncols, U, ldU, Tg, X, ldX, st);
+}
+
 template <bool FWD, bool PRE>
 int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
               long ldX, cudaStream_t st) {
@@ -505,10 +711,10 @@ int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double
   if (tbuf) {
     if (forward) {
       EVD_TRY(launch_tbuild<true>(n, U, ldU, tbuf, st));
-      return launch_q2<true, true>(n, ncols, U, ldU, tbuf, X, ldX, st);
+      return launch_q2_pre<true>(n, ncols, U, ldU, tbuf, X, ldX, st);
     }
     EVD_TRY(launch_tbuild<false>(n, U, ldU, tbuf, st));
-    return launch_q2<false, true>(n, ncols, U, ldU, tbuf, X, ldX, st);
+    return launch_q2_pre<false>(n, ncols, U, ldU, tbuf, X, ldX, st);
   }
   return forward ? launch_q2<true, false>(n, ncols, U, ldU, nullptr, X, ldX, st)
                  : launch_q2<false, false>(n, ncols, U, ldU, nullptr, X, ldX, st);
