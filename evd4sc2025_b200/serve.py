@@ -1,7 +1,7 @@
 """Batched uneven-size solves and a continuous-batching serving loop.
 
-Both sit on the plain FP64 solver (``evd_syevd``).  The reference solves one
-matrix per process (``myEVD n b nb``, src/EVD/myEVD.cu:251-706, n a multiple
+Both sit on the solvers of this library (``evd_syevd``, ``evd_syevd_mixed``).
+The reference solves one matrix per process (``myEVD n b nb``, src/EVD/myEVD.cu:251-706, n a multiple
 of 1024); this layer adds:
 
 * **any n >= 1** through ``evd_syevd`` itself, which pads an order that is
@@ -22,8 +22,12 @@ of 1024); this layer adds:
   frees up.  Latency = completion - arrival; the server reports solves/s and
   p50/p99 latency.
 
-Every request is served by the FP64 solver, so FP32-tolerance requests get
-FP64 accuracy (the mixed-precision path is not part of this library).
+Requests carry an accuracy class (:func:`request_form`): FP64-accurate
+requests of order >= ``MIXED_MIN_N`` are solved by the mixed form
+(``evd_syevd_mixed``, emulated FP64 products with 14 moduli), FP32-tolerance
+requests of that size by the mixed form with 8 moduli (30-bit operands, no
+refinement: eigenpairs to about 1e-8), and smaller requests of either class
+by the plain FP64 solver, which is faster there.
 """
 from __future__ import annotations
 
@@ -65,11 +69,34 @@ def solve_shape(n: int) -> tuple[int, int]:
     return autotune.padded_order(n, nb), nb
 
 
-def footprint_bytes(n: int) -> int:
+FP64_MODULI = 14   # emulated products with 53-bit operands: FP64-level
+FP32_MODULI = 8    # 30-bit operands: the FP32-tolerance class (residual <= 1e-6)
+MIXED_MIN_N = 2048  # below it the plain FP64 solver is faster than the mixed form
+
+
+def request_form(n: int, tol: str = "fp64") -> tuple[str, int]:
+    """("plain", 0) or ("mixed", moduli) for a request of order n and
+    accuracy class ``tol`` ("fp64": residual <= 1e-13, "fp32": <= 1e-6)."""
+    if tol not in ("fp64", "fp32"):
+        raise ValueError(f"unknown accuracy class {tol!r}")
+    if n < MIXED_MIN_N:
+        return "plain", 0
+    return "mixed", FP64_MODULI if tol == "fp64" else FP32_MODULI
+
+
+def work_bytes(n: int, nb: int, tol: str = "fp64") -> int:
+    """Workspace bytes of the solve :func:`request_form` picks."""
+    form, mod = request_form(n, tol)
+    if form == "plain":
+        return int(lib().evd_syevd_work_size(n, 32, nb))
+    return int(lib().evd_syevd_mixed_work_size(n, 32, nb, mod, 0))
+
+
+def footprint_bytes(n: int, tol: str = "fp64") -> int:
     """Device bytes one solve of order n holds: workspace (with the padded
     copies when n' > n) + A and X of order n + w."""
     _, nb = solve_shape(n)
-    return int(lib().evd_syevd_work_size(n, 32, nb)) + 2 * n * n * 8 + n * 8
+    return work_bytes(n, nb, tol) + 2 * n * n * 8 + n * 8
 
 
 class StreamSolver:
@@ -87,8 +114,8 @@ class StreamSolver:
         self._ld = 0
         self._A = None
 
-    def _ensure(self, n: int, nb: int):
-        need = int(lib().evd_syevd_work_size(n, 32, nb))
+    def _ensure(self, n: int, nb: int, tol: str = "fp64"):
+        need = work_bytes(n, nb, tol)
         if need <= 0:
             raise ValueError(f"unsupported order {n} (nb {nb})")
         if need > self._wsbytes:
@@ -106,14 +133,26 @@ class StreamSolver:
         self._ws = self._A = None
         self._wsbytes = self._ld = 0
 
-    def solve(self, A: torch.Tensor, nb: int | None = None):
+    def solve(self, A: torch.Tensor, nb: int | None = None, tol: str = "fp64",
+              plain: bool = False):
         """Eigenvalues (ascending, length n) and eigenvectors (n x n,
-        column-major) of the symmetric FP64 matrix A on this worker's stream.
-        A may live on the host or the device; results are on the device.
-        The padding runs on the device; the solver's own host reads are its
-        only synchronisation.  ``nb`` overrides the block size of
+        column-major) of the symmetric FP64 matrix A on this worker's stream,
+        by the form :func:`request_form` picks for the accuracy class ``tol``
+        (``plain``: the plain FP64 solver whatever the class).  A may live on
+        the host or the device; results are on the device.  The padding runs
+        on the device; the solver's own host reads are its only
+        synchronisation.  ``nb`` overrides the block size of
         :func:`solve_shape`."""
         n = A.shape[0]
+        form, mod = ("plain", 0) if plain else request_form(n, tol)
+        if plain:
+            tol = "fp64"
+            if n >= MIXED_MIN_N:  # work_bytes sizes by the class: ask for the plain size
+                need = int(lib().evd_syevd_work_size(n, 32, nb or solve_shape(n)[1]))
+                if need > self._wsbytes:
+                    self._ws = None
+                    self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+                    self._wsbytes = need
         if nb is None:
             _, nb = solve_shape(n)
         # The results belong to the caller's stream; the solve runs on this
@@ -130,12 +169,16 @@ class StreamSolver:
         if A.is_cuda:
             A.record_stream(self.stream)
         with torch.cuda.stream(self.stream):
-            Ab = self._ensure(n, nb)
+            Ab = self._ensure(n, nb, tol)
             Ab.copy_(A, non_blocking=True)
             pa, lda = _cm(Ab, "A")
             px, ldx = _cm(X, "X")
-            call("evd_syevd", n, 32, nb, pa, lda, _ptr(w), px, ldx, _ptr(self._ws),
-                 self._wsbytes, 0, _stream(self.stream))
+            if form == "plain":
+                call("evd_syevd", n, 32, nb, pa, lda, _ptr(w), px, ldx, _ptr(self._ws),
+                     self._wsbytes, 0, _stream(self.stream))
+            else:
+                call("evd_syevd_mixed", n, 32, nb, pa, lda, _ptr(w), px, ldx, mod, 0,
+                     FP64_MODULI, _ptr(self._ws), self._wsbytes, 0, _stream(self.stream))
         return w, X
 
 
@@ -252,6 +295,7 @@ class Result:
     w: torch.Tensor | None
     X: torch.Tensor | None
     error: str | None = None           # set when the solve failed (w, X are None)
+    tol: str = "fp64"
 
     @property
     def latency(self) -> float:
@@ -267,8 +311,11 @@ class Server:
     free worker; its footprint is returned when its solve completes.  Results
     keep the eigenpairs on the host (``to_host``) or the device.
 
-    ``solve_fn(worker_index, A) -> (w, X)`` and ``footprint_fn(n)`` can be
-    replaced (the tests drive the admission logic without a GPU).  The budget
+    ``solve_fn(worker_index, A, tol) -> (w, X)`` and ``footprint_fn(n, tol)``
+    can be replaced (the tests drive the admission logic without a GPU).
+    ``keep(request) -> bool`` selects the requests whose eigenpairs are kept
+    in the results (all by default; the others count in the statistics and
+    release their memory as soon as they are solved).  The budget
     bounds the sum of the footprints of admitted requests; each worker also
     keeps the buffers of the largest problem it has solved, so the device
     holds at most that sum plus one largest footprint per worker.
@@ -276,16 +323,17 @@ class Server:
 
     def __init__(self, nworkers: int = 8, budget_bytes: int = 150 * 10**9, device="cuda",
                  solve_fn: Callable | None = None, footprint_fn: Callable | None = None,
-                 to_host: bool = True):
+                 to_host: bool = True, keep: Callable | None = None):
         self.nworkers = nworkers
         self.budget = budget_bytes
         self.to_host = to_host
+        self.keep = keep or (lambda req: True)
         self.footprint_fn = footprint_fn or footprint_bytes
         if solve_fn is None:
             self._solvers = [StreamSolver(device) for _ in range(nworkers)]
 
-            def solve_fn(k, A):
-                w, X = self._solvers[k].solve(A)
+            def solve_fn(k, A, tol):
+                w, X = self._solvers[k].solve(A, tol=tol)
                 if self.to_host:
                     w, X = w.cpu(), X.cpu()  # synchronises the worker's stream
                 else:
@@ -309,15 +357,17 @@ class Server:
                 _, _, req, t_adm = heapq.heappop(self._ready)
             err = None
             try:
-                w, X = self.solve_fn(k, req.A)
+                w, X = self.solve_fn(k, req.A, req.tol)
             except Exception as e:  # a failed request must still return its memory
                 w = X = None
                 err = f"{type(e).__name__}: {e}"
             t_done = time.perf_counter() - t0
+            if not self.keep(req):
+                w = X = None
             with self._cv:
                 self._in_use -= req.bytes
                 self._results.append(Result(req.rid, req.A.shape[0], req.arrival, t_adm, t_done,
-                                            w, X, err))
+                                            w, X, err, req.tol))
                 self._cv.notify_all()
 
     def run(self, requests: list[Request]) -> dict:
@@ -332,7 +382,7 @@ class Server:
             self.max_in_flight_bytes = 0
         reqs = sorted(requests)
         for r in reqs:
-            r.bytes = int(self.footprint_fn(r.A.shape[0]))
+            r.bytes = int(self.footprint_fn(r.A.shape[0], r.tol))
             if r.bytes > self.budget:
                 raise ValueError(f"request {r.rid} (n={r.A.shape[0]}) needs {r.bytes} bytes, "
                                  f"more than the budget {self.budget}")
@@ -361,14 +411,20 @@ class Server:
         wall = time.perf_counter() - t0
         lat = sorted(res.latency for res in self._results)
 
-        def pct(p):
-            if not lat:
+        def pct(vals, p):
+            if not vals:
                 return float("nan")
-            return lat[min(len(lat) - 1, int(math.ceil(p / 100.0 * len(lat))) - 1)]
+            return vals[min(len(vals) - 1, int(math.ceil(p / 100.0 * len(vals))) - 1)]
+        per_class = {}
+        for c in ("fp64", "fp32"):
+            lc = sorted(res.latency for res in self._results if res.tol == c)
+            if lc:
+                per_class[c] = {"requests": len(lc), "p50_s": pct(lc, 50), "p99_s": pct(lc, 99)}
         return {"requests": len(self._results), "wall_s": wall,
                 "failed": sum(1 for r in self._results if r.error is not None),
                 "solves_per_s": len(self._results) / wall if wall > 0 else float("nan"),
-                "p50_s": pct(50), "p99_s": pct(99), "max_in_flight_bytes": self.max_in_flight_bytes}
+                "p50_s": pct(lat, 50), "p99_s": pct(lat, 99), "per_class": per_class,
+                "max_in_flight_bytes": self.max_in_flight_bytes}
 
     @property
     def results(self) -> list[Result]:

@@ -81,3 +81,46 @@ def test_server_mix_matches_alone(cuda, evdlib):
         nrm = float(torch.linalg.matrix_norm(r.A, ord=2))
         assert float((res.w - w1.cpu()).abs().max()) <= 1e-13 * nrm
         _check(r.A, res.w, res.X)
+
+
+def _check_class(A, w, X, tol):
+    A = A.numpy()
+    w = w.cpu().numpy()
+    X = X.cpu().numpy()
+    n = A.shape[0]
+    res = np.linalg.norm(A @ X - X * w) / (n * np.linalg.norm(A))
+    orth = np.linalg.norm(X.T @ X - np.eye(n)) / n
+    bar = 1e-13 if tol == "fp64" else 1e-6
+    assert res <= bar and orth <= bar, (tol, res, orth)
+    nrm = np.linalg.norm(A, 2)
+    ebar = 1e-12 if tol == "fp64" else 1e-6
+    assert np.abs(np.sort(w) - np.linalg.eigvalsh(A)).max() <= ebar * nrm
+
+
+def test_server_two_classes_mix_matches_alone(cuda, evdlib):
+    """FP64-accurate and FP32-tolerance requests, some large enough for the
+    mixed form: each result in the mix equals the same request solved alone
+    by the same form, and meets its class's bars."""
+    reqs = serve.poisson_stream(10, 200.0, 1200, 3000, seed=21, fp64_fraction=0.6)
+    assert {r.tol for r in reqs} == {"fp64", "fp32"}
+    assert any(r.A.shape[0] >= serve.MIXED_MIN_N for r in reqs)
+    srv = serve.Server(nworkers=3, budget_bytes=40 * 10**9, device=cuda)
+    stats = srv.run(reqs)
+    assert stats["requests"] == len(reqs) and stats["failed"] == 0
+    assert set(stats["per_class"]) == {"fp64", "fp32"}
+    alone = serve.StreamSolver(cuda)
+    for r, res in zip(sorted(reqs, key=lambda q: q.rid), srv.results):
+        assert r.rid == res.rid and res.tol == r.tol
+        w1, X1 = alone.solve(r.A.to(cuda), tol=r.tol)
+        alone.stream.synchronize()
+        nrm = float(torch.linalg.matrix_norm(r.A, ord=2))
+        assert float((res.w - w1.cpu()).abs().max()) <= 1e-13 * nrm
+        _check_class(r.A, res.w, res.X, r.tol)
+
+
+def test_request_form_rule(evdlib):
+    assert serve.request_form(1000, "fp64") == ("plain", 0)
+    assert serve.request_form(4096, "fp64") == ("mixed", serve.FP64_MODULI)
+    assert serve.request_form(4096, "fp32") == ("mixed", serve.FP32_MODULI)
+    with pytest.raises(ValueError):
+        serve.request_form(4096, "fp16")

@@ -45,7 +45,7 @@ def test_admission_respects_budget_and_serves_everything():
     in_flight = {"now": 0, "max": 0}
     lock = threading.Lock()
 
-    def solve(k, A):
+    def solve(k, A, tol):
         n = A.shape[0]
         with lock:
             in_flight["now"] += n
@@ -56,7 +56,7 @@ def test_admission_respects_budget_and_serves_everything():
         return torch.zeros(n), torch.zeros(n, n)
 
     sizes = [30, 50, 20, 70, 10, 40, 60, 25, 35, 45]
-    srv = serve.Server(nworkers=4, budget_bytes=100, solve_fn=solve, footprint_fn=lambda n: n)
+    srv = serve.Server(nworkers=4, budget_bytes=100, solve_fn=solve, footprint_fn=lambda n, tol: n)
     stats = srv.run(_fake_requests(sizes))
     assert stats["requests"] == len(sizes)
     assert srv.max_in_flight_bytes <= 100
@@ -69,8 +69,8 @@ def test_admission_respects_budget_and_serves_everything():
 
 
 def test_oversized_request_is_rejected():
-    srv = serve.Server(nworkers=1, budget_bytes=10, solve_fn=lambda k, A: (None, None),
-                       footprint_fn=lambda n: n)
+    srv = serve.Server(nworkers=1, budget_bytes=10, solve_fn=lambda k, A, tol: (None, None),
+                       footprint_fn=lambda n, tol: n)
     with pytest.raises(ValueError):
         srv.run(_fake_requests([5, 11]))
 
@@ -129,8 +129,8 @@ def test_autotune_active_table_switch():
 def test_server_runs_twice():
     """A server can serve a second stream after the first (warm-up, then the
     measured stream); results and statistics are per run."""
-    srv = serve.Server(nworkers=2, budget_bytes=100, solve_fn=lambda k, A: (A, A),
-                       footprint_fn=lambda n: n)
+    srv = serve.Server(nworkers=2, budget_bytes=100, solve_fn=lambda k, A, tol: (A, A),
+                       footprint_fn=lambda n, tol: n)
     first = srv.run(_fake_requests([3, 4, 5], gap=0.0))
     assert first["requests"] == 3
     second = srv.run(_fake_requests([6, 7], gap=0.0))
@@ -140,11 +140,11 @@ def test_server_runs_twice():
 def test_failed_solve_returns_its_memory():
     """A request whose solve raises is reported as failed and gives its memory
     back, so the requests behind it are still admitted and served."""
-    def solve(k, A):
+    def solve(k, A, tol):
         if A.shape[0] == 5:
             raise RuntimeError("bad input")
         return A, A
-    srv = serve.Server(nworkers=1, budget_bytes=6, solve_fn=solve, footprint_fn=lambda n: n)
+    srv = serve.Server(nworkers=1, budget_bytes=6, solve_fn=solve, footprint_fn=lambda n, tol: n)
     stats = srv.run(_fake_requests([5, 6, 4, 6], gap=0.0))
     assert stats["requests"] == 4 and stats["failed"] == 1
     bad = [r for r in srv.results if r.error is not None]
