@@ -158,7 +158,7 @@ struct ChaseSmem {
 
 __global__ void __launch_bounds__(kChaseThreads)
     chase_kernel(int n, double* __restrict__ sub, double* __restrict__ U, long ldU, int* prog,
-                 int* ticket, int* err) {
+                 int* ticket, int* err, int s_begin, int s_end) {
   __shared__ __align__(16) ChaseSmem sm;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
@@ -167,14 +167,14 @@ __global__ void __launch_bounds__(kChaseThreads)
 
   for (;;) {
     if (tid == 0) {
-      int t = atomicAdd(ticket, 1);
+      int t = s_begin + atomicAdd(ticket, 1);
       if (*(volatile int*)err != 0) t = n;  // drain after an error elsewhere
       sm.ticket = t;
     }
     __syncthreads();
     const int s = sm.ticket;
     __syncthreads();
-    if (s >= n - 2) break;
+    if (s >= s_end) break;
 
     long r = s + 1;
     int rb = min(kBW, (int)(n - r));
@@ -303,9 +303,16 @@ __global__ void __launch_bounds__(kChaseThreads)
       rb = rb2;
       r = r2;
       cur = 1 - cur;
-      if (s > 0 && !cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) {
-        alive = false;
-        break;
+      // the next step's Householder warp reads B1 = this step's B1', written
+      // by all four warps in (6): the wait below ends with a CTA barrier; sweep
+      // 0 waits on nobody and takes the barrier alone
+      if (s > 0) {
+        if (!cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) {
+          alive = false;
+          break;
+        }
+      } else {
+        __syncthreads();
       }
     }
     if (!alive) break;
@@ -346,6 +353,49 @@ int band_pack(long n, long b, const double* dA, long ldA, double* dSub, long ldS
 
 long chase_iwork_ints(long n) { return n + 64; }
 
+// Sweeps [s0, s1) of the chase as one launch (part `part`, 0 <= part < 32, of
+// a chase split into consecutive ranges; part 0 starts at s0 = 0 and clears
+// the flags, tickets and error word).  Each part has its own ticket counter
+// (iwork[n + part]); a part's first sweep waits on the previous sweep's
+// progress flag, which the previous part's launch left at its final value.
+// Splitting costs one pipeline drain per part boundary: the next part's
+// first sweep starts when the previous sweep has reached the end of the band,
+// not 2b rows after its start.
+int chase_part_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU, int* iwork,
+                     long s0, long s1, int part, cudaStream_t st) {
+  if (n < 0 || b != kBW || ldSub != 2 * b || (dU && n > 0 && ldU < n)) return EVD_ERR_INVALID_ARG;
+  if (((uintptr_t)dSub & 15u) != 0) return EVD_ERR_INVALID_ARG;
+  if (n > (1L << 30)) return EVD_ERR_INVALID_ARG;
+  if (part < 0 || part >= 32 || s0 < 0 || s1 < s0 || (part == 0) != (s0 == 0))
+    return EVD_ERR_INVALID_ARG;
+  if (n == 0) return EVD_SUCCESS;
+  if (!dSub || !iwork) return EVD_ERR_INVALID_ARG;
+  int* prog = iwork;
+  int* err = iwork + n + 32;
+  if (part == 0) EVD_CUDA_TRY(cudaMemsetAsync(iwork, 0, sizeof(int) * chase_iwork_ints(n), st));
+  s1 = std::min(s1, n - 2);
+  if (s1 > s0) {
+    // enough CTAs for the pipeline's concurrency (a sweep starts every 3 steps
+    // and lasts about n/b steps), bounded by the GPU's resident capacity
+    const long sweeps = s1 - s0;
+    const long want = n / (3 * kBW) + 16;
+    const int ctas = (int)std::min(std::min(sweeps, want), 6L * device_sm_count());
+    chase_kernel<<<ctas, kChaseThreads, 0, st>>>((int)n, dSub, dU, ldU, prog, iwork + n + part,
+                                                 err, (int)s0, (int)s1);
+    EVD_LAUNCHED();
+  }
+  return EVD_SUCCESS;
+}
+
+// d and e from the chased band (after the last part).
+int chase_tridiag(long n, const double* dSub, long ldSub, double* d, double* e, cudaStream_t st) {
+  if (n <= 0) return EVD_SUCCESS;
+  if (!dSub || !d || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;
+  band_to_tridiag_kernel<<<ceil_div_i(n, 256), 256, 0, st>>>((int)n, dSub, ldSub, d, e);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
 // Launch the chase; does not synchronise.  iwork: chase_iwork_ints(n) ints.
 // The error word is iwork[n + 32] (0 = ok).
 // The tile copies need ldSub == 2b exactly (contiguous band columns) and a
@@ -357,22 +407,8 @@ int bulge_chase_async(long n, long b, double* dSub, long ldSub, double* dU, long
   if (n > (1L << 30)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (!dSub || !d || !iwork || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;  // dU may be NULL
-  int* prog = iwork;
-  int* ticket = iwork + n;
-  int* err = iwork + n + 32;
-  EVD_CUDA_TRY(cudaMemsetAsync(iwork, 0, sizeof(int) * chase_iwork_ints(n), st));
-  if (n > 2) {
-    // enough CTAs for the pipeline's concurrency (a sweep starts every 3 steps
-    // and lasts about n/b steps), bounded by the GPU's resident capacity
-    const long sweeps = n - 2;
-    const long want = n / (3 * kBW) + 16;
-    const int ctas = (int)std::min(std::min(sweeps, want), 6L * device_sm_count());
-    chase_kernel<<<ctas, kChaseThreads, 0, st>>>((int)n, dSub, dU, ldU, prog, ticket, err);
-    EVD_LAUNCHED();
-  }
-  band_to_tridiag_kernel<<<ceil_div_i(n, 256), 256, 0, st>>>((int)n, dSub, ldSub, d, e);
-  EVD_LAUNCHED();
-  return EVD_SUCCESS;
+  EVD_TRY(chase_part_async(n, b, dSub, ldSub, dU, ldU, iwork, 0, n - 2, 0, st));
+  return chase_tridiag(n, dSub, ldSub, d, e, st);
 }
 
 int read_device_error(const int* err_word, cudaStream_t st) {
