@@ -456,12 +456,14 @@ def syevd_mixed(A: torch.Tensor, b: int = 32, nb: int = 1024, moduli: int = 14,
 
 def mixed_last_timings() -> dict:
     """Stage times (ms) of the last timed :func:`syevd_mixed` on this thread.
-    q1_formation and stage2_on_q1t run on a side stream beside the chase and
-    the divide and conquer; x_eq_qz includes waiting for them."""
+    q1_formation and stage2_chains (the stage-2 reflectors accumulated from the
+    identity, one chase range behind the chase) run on side streams beside the
+    chase and the divide and conquer; final_products (from the end of the
+    divide and conquer to X) includes waiting for them."""
     out = (C.c_double * 8)()
     lib().evd_syevd_mixed_last_timings(out)
-    keys = ("sy2sb", "bulge_chasing", "tridiagonal_dc", "q1_formation", "stage2_on_q1t",
-            "x_eq_qz", "refine", "total")
+    keys = ("sy2sb", "bulge_chasing", "tridiagonal_dc", "q1_formation", "stage2_chains",
+            "final_products", "refine", "total")
     return {k: float(v) for k, v in zip(keys, out)}
 
 

@@ -231,14 +231,36 @@ __host__ __device__ __forceinline__ long tblock(long s, long bb, long B0) {
   return s * B0 - 8 * s * (s - 1) + bb;
 }
 
+// Sweeps [h0, h1) of the chase (h0 a multiple of 8; h1 a multiple of 8 or at
+// least n - 2): the blocks of those sweeps in every strip.  Splitting the
+// sweeps into consecutive ranges, each applied to all strips, keeps the
+// generation order: every reflector of a range precedes, in that order,
+// every reflector of a later range that it overlaps.
+// ident (forward only): X was the identity before sweep k = ident_k (k <= h0).
+// Then column c is zero below row c + 30 + (h - k) before sweep h (each sweep
+// moves the lowest nonzero row of a column down by at most one after the
+// first), and sweep h touches rows >= R + h + 1 of strip R, so a strip with
+// R > c + 29 - k never meets a nonzero of column c: a CTA skips the strips
+// that lie wholly below its columns (with a margin of 64 rows).
+struct Q2Range {
+  int h0, h1, ident, ident_k;
+  int rev;  // CTA b takes column block gridDim.x - 1 - b (the heaviest first)
+};
+
+__host__ __device__ __forceinline__ bool q2_skip_strip(const Q2Range& rg, long R, long cta_col0,
+                                                       int cta_cols) {
+  return rg.ident && R > cta_col0 + cta_cols + 64 - rg.ident_k;
+}
+
 // -V fragments of every block of every strip (one CTA per block, one warp
 // per group), in the layout the apply kernel reads.
 template <bool FWD>
 __global__ void __launch_bounds__(kQThreads)
-    q2_tbuild_kernel(int n, const double* __restrict__ U, long ldU, double* __restrict__ Tg) {
+    q2_tbuild_kernel(int n, const double* __restrict__ U, long ldU, double* __restrict__ Tg,
+                     int bb0) {
   __shared__ __align__(16) double ys[kYBuf];
   __shared__ double gsh[kQW * kGBuf];
-  const int s = blockIdx.y, bb = blockIdx.x;
+  const int s = blockIdx.y, bb = bb0 + (int)blockIdx.x;
   const int B0 = (n - 2 + 7) / 8;
   const int nblk = B0 - (kStrip / 8) * s;
   if (bb >= nblk) return;
@@ -356,11 +378,12 @@ __device__ __forceinline__ void store_tile(const double (&v)[4], const TileIO& i
 
 // PRE: the -T fragments were precomputed into Tg by q2_tbuild_kernel and are
 // staged with the reflectors; otherwise each block's T is built here, one
-// block ahead, by the same warps.
+// block ahead, by the same warps.  rg restricts the kernel to a range of
+// sweeps (and marks an identity start, see Q2Range).
 template <bool FWD, bool PRE>
 __global__ void __launch_bounds__(kQThreads, 2)
     q2_mma_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
-                  const double* __restrict__ Tg, double* __restrict__ X, long ldX) {
+                  const double* __restrict__ Tg, double* __restrict__ X, long ldX, Q2Range rg) {
   extern __shared__ __align__(16) double smem[];
   double* Ys = smem;                 // kNYBuf x kYBuf
   double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kVBuf (PRE: -V) or 2 x kTBuf (-T)
@@ -378,7 +401,8 @@ __global__ void __launch_bounds__(kQThreads, 2)
   const int offU0 = seg_off(2 * t, 0) + g - 2 * t;          // Y[8i+g][2t]
   const int offU1 = seg_off(2 * t + 1, 0) + g - 2 * t - 1;  // Y[8i+g][2t+1]
 
-  const int c0 = blockIdx.x * (kQW * kQCols) + warp * kQCols;
+  const int cblk = rg.rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int c0 = cblk * (kQW * kQCols) + warp * kQCols;
   TileIO io;
   io.okg = c0 + g < ncols;
   io.okg8 = c0 + g + 8 < ncols;
@@ -394,12 +418,16 @@ __global__ void __launch_bounds__(kQThreads, 2)
     const double* src = Tg + tblock(sidx, bb, B0) * kVBuf;
     for (int e = threadIdx.x; e < kVBuf / 2; e += kQThreads) cp_async16(dst + 2 * e, src + 2 * e);
   };
+  const long cta_col0 = (long)cblk * (kQW * kQCols);
   for (int si = 0; si < nstrips; ++si) {
     const int sidx = FWD ? (nstrips - 1 - si) : si;
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;  // sweeps with reflectors in this strip
     const int nblk = (H + 7) / 8;
-    auto bb_of = [&](int it) { return FWD ? it : (nblk - 1 - it); };
+    const int bbA = rg.h0 / 8, bbB = min(nblk, (rg.h1 + 7) / 8);
+    const int cnt = bbB - bbA;  // blocks of this launch's sweeps in the strip
+    if (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, kQW * kQCols)) continue;
+    auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();  // previous strip done with Ys / Ts; zero fill visible
     {
@@ -410,7 +438,7 @@ __global__ void __launch_bounds__(kQThreads, 2)
     stage_block(Ys, U, ldU, n, R, H, bb_of(0));
     if (PRE) stage_t(Ts, sidx, bb_of(0));
     cp_commit();
-    if (nblk > 1) {
+    if (cnt > 1) {
       stage_block(Ys + kYBuf, U, ldU, n, R, H, bb_of(1));
       if (PRE) stage_t(Ts + kVBuf, sidx, bb_of(1));
     }
@@ -420,12 +448,12 @@ __global__ void __launch_bounds__(kQThreads, 2)
     if (!PRE) build_t<FWD>(Ys, Ts, gs, warp, lane, offW);
 
 #pragma unroll 1
-    for (int it = 0; it < nblk; ++it) {
+    for (int it = 0; it < cnt; ++it) {
       const int bb = bb_of(it);
       const long base = R + 8L * bb + 1;
       cp_wait<0>();
       __syncthreads();  // block it+1 staged; T of block it complete
-      if (it + 2 < nblk) {
+      if (it + 2 < cnt) {
         stage_block(Ys + ((it + 2) % 3) * kYBuf, U, ldU, n, R, H, bb_of(it + 2));
         if (PRE) stage_t(Ts + ((it + 2) % 3) * kVBuf, sidx, bb_of(it + 2));
       }
@@ -434,7 +462,7 @@ __global__ void __launch_bounds__(kQThreads, 2)
       load_tile(inc, io, FWD ? (base + 8 * kTiles) : (base - 8), n);
       const double* ys = Ys + (it % 3) * kYBuf;
       const double* ts = Ts + (PRE ? (it % 3) * kVBuf : (it & 1) * kTBuf);
-      if (!PRE && it + 1 < nblk)
+      if (!PRE && it + 1 < cnt)
         build_t<FWD>(Ys + ((it + 1) % 3) * kYBuf, Ts + ((it + 1) & 1) * kTBuf, gs, warp, lane,
                      offW);
       apply_block<FWD, PRE>(x, ys, ts, lane, offW, offU0, offU1);
@@ -459,7 +487,7 @@ __global__ void __launch_bounds__(kQThreads, 2)
     }
     // the window now holds the frame one block past the last one
     {
-      const long base = FWD ? (R + 8L * nblk + 1) : (R - 7);
+      const long base = FWD ? (R + 8L * bbB + 1) : (R + 8L * bbA - 7);
 #pragma unroll
       for (int i = 0; i < kTiles; ++i) store_tile(x[i], io, base + 8 * i, n);
     }
@@ -545,7 +573,7 @@ __device__ __forceinline__ void store_tile8(const double (&v)[2], double* cg, bo
 template <bool FWD, int NW>
 __global__ void __launch_bounds__(NW * 32, 2)
     q2_mma8_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
-                   const double* __restrict__ Tg, double* __restrict__ X, long ldX) {
+                   const double* __restrict__ Tg, double* __restrict__ X, long ldX, Q2Range rg) {
   extern __shared__ __align__(16) double smem[];
   double* Ys = smem;                 // kNYBuf x kYBuf
   double* Ts = Ys + kNYBuf * kYBuf;  // kNYBuf x kVBuf (-V fragments)
@@ -554,7 +582,8 @@ __global__ void __launch_bounds__(NW * 32, 2)
   const int g = lane >> 2, t = lane & 3;
   for (int e = threadIdx.x; e < kNYBuf * kYBuf; e += nthr) Ys[e] = 0.0;
   const int offW = seg_off(g, 0) + 2 * t - g;  // Y[8i+2t(+1)][g]
-  const int c0 = blockIdx.x * (NW * kQ8Cols) + warp * kQ8Cols;
+  const int cblk = rg.rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int c0 = cblk * (NW * kQ8Cols) + warp * kQ8Cols;
   const bool okg = c0 + g < ncols;
   double* cg = X + (long)(okg ? c0 + g : 0) * ldX;
   const int t2 = 2 * t;
@@ -576,12 +605,16 @@ __global__ void __launch_bounds__(NW * 32, 2)
     const double* src = Tg + tblock(sidx, bb, B0) * kVBuf;
     for (int e = threadIdx.x; e < kVBuf / 2; e += nthr) cp_async16(dst + 2 * e, src + 2 * e);
   };
+  const long cta_col0 = (long)cblk * (NW * kQ8Cols);
   for (int si = 0; si < nstrips; ++si) {
     const int sidx = FWD ? (nstrips - 1 - si) : si;
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;
     const int nblk = (H + 7) / 8;
-    auto bb_of = [&](int it) { return FWD ? it : (nblk - 1 - it); };
+    const int bbA = rg.h0 / 8, bbB = min(nblk, (rg.h1 + 7) / 8);
+    const int cnt = bbB - bbA;
+    if (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, NW * kQ8Cols)) continue;
+    auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();
     {
@@ -592,7 +625,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
     stage_y(Ys, R, H, bb_of(0));
     stage_t(Ts, sidx, bb_of(0));
     cp_commit();
-    if (nblk > 1) {
+    if (cnt > 1) {
       stage_y(Ys + kYBuf, R, H, bb_of(1));
       stage_t(Ts + kVBuf, sidx, bb_of(1));
     }
@@ -601,12 +634,12 @@ __global__ void __launch_bounds__(NW * 32, 2)
     __syncthreads();
 
 #pragma unroll 1
-    for (int it = 0; it < nblk; ++it) {
+    for (int it = 0; it < cnt; ++it) {
       const int bb = bb_of(it);
       const long base = R + 8L * bb + 1;
       cp_wait<0>();
       __syncthreads();
-      if (it + 2 < nblk) {
+      if (it + 2 < cnt) {
         stage_y(Ys + ((it + 2) % 3) * kYBuf, R, H, bb_of(it + 2));
         stage_t(Ts + ((it + 2) % 3) * kVBuf, sidx, bb_of(it + 2));
       }
@@ -635,7 +668,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
       }
     }
     {
-      const long base = FWD ? (R + 8L * nblk + 1) : (R - 7);
+      const long base = FWD ? (R + 8L * bbB + 1) : (R + 8L * bbA - 7);
 #pragma unroll
       for (int i = 0; i < kTiles; ++i) store_tile8(x[i], cg, okg, base + 8 * i, t2, n);
     }
@@ -646,17 +679,18 @@ constexpr size_t kQ8Smem = (size_t)(kNYBuf * kYBuf + kNYBuf * kVBuf) * sizeof(do
 
 template <bool FWD, int NW>
 int launch_q2_8(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-                long ldX, cudaStream_t st) {
+                long ldX, Q2Range rg, cudaStream_t st) {
   EVD_TRY(smem_attr_once((const void*)q2_mma8_kernel<FWD, NW>, (int)kQ8Smem));
   const int grid = ceil_div_i((int)ncols, NW * kQ8Cols);
-  q2_mma8_kernel<FWD, NW><<<grid, NW * 32, kQ8Smem, st>>>((int)n, (int)ncols, U, ldU, Tg, X, ldX);
+  q2_mma8_kernel<FWD, NW><<<grid, NW * 32, kQ8Smem, st>>>((int)n, (int)ncols, U, ldU, Tg, X, ldX,
+                                                          rg);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
 template <bool FWD, bool PRE>
 int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-              long ldX, cudaStream_t st);
+              long ldX, Q2Range rg, cudaStream_t st);
 
 // With fewer 64-column CTAs than SMs (ncols < 64 x SMs: n <= 8192 on B200)
 // the 16-column kernel leaves SMs idle; the 8-column kernel (4 warps, 32
@@ -666,28 +700,32 @@ int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, d
 // flop).
 template <bool FWD>
 int launch_q2_pre(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-                  long ldX, cudaStream_t st) {
+                  long ldX, Q2Range rg, cudaStream_t st) {
   if (ncols >= 64L * device_sm_count())
-    return launch_q2<FWD, true>(n, ncols, U, ldU, Tg, X, ldX, st);
-  return launch_q2_8<FWD, 4>(n, ncols, U, ldU, Tg, X, ldX, st);
+    return launch_q2<FWD, true>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
+  return launch_q2_8<FWD, 4>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
 }
 
 template <bool FWD, bool PRE>
 int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-              long ldX, cudaStream_t st) {
+              long ldX, Q2Range rg, cudaStream_t st) {
   EVD_TRY(smem_attr_once((const void*)q2_mma_kernel<FWD, PRE>, (int)kQSmem));
   int grid = ceil_div_i((int)ncols, kQW * kQCols);
   q2_mma_kernel<FWD, PRE><<<grid, kQThreads, kQSmem, st>>>((int)n, (int)ncols, U, ldU, Tg, X,
-                                                           ldX);
+                                                           ldX, rg);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
+// -V fragments of the blocks of sweeps [h0, h1) in every strip.
 template <bool FWD>
-int launch_tbuild(long n, const double* U, long ldU, double* Tg, cudaStream_t st) {
+int launch_tbuild(long n, const double* U, long ldU, double* Tg, long h0, long h1,
+                  cudaStream_t st) {
   const int nstrips = (int)((n - 2 + kStrip - 1) / kStrip);
   const int B0 = (int)((n - 2 + 7) / 8);
-  q2_tbuild_kernel<FWD><<<dim3(B0, nstrips), kQThreads, 0, st>>>((int)n, U, ldU, Tg);
+  const int bbA = (int)(h0 / 8), bbB = (int)std::min<long>(B0, (h1 + 7) / 8);
+  if (bbB <= bbA) return EVD_SUCCESS;
+  q2_tbuild_kernel<FWD><<<dim3(bbB - bbA, nstrips), kQThreads, 0, st>>>((int)n, U, ldU, Tg, bbA);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
@@ -701,23 +739,35 @@ long q2_tbuf_doubles(long n) {
   return tblock(nstrips, 0, B0) * kVBuf;
 }
 
-int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
-             double* tbuf, cudaStream_t st) {
+int q2_apply_range(bool forward, long n, long ncols, const double* U, long ldU, double* X,
+                   long ldX, double* tbuf, long h0, long h1, long ident_k, cudaStream_t st) {
+  const bool ident = ident_k >= 0;
   if (n < 0 || ncols < 0 || ldU < n || ldX < n) return EVD_ERR_INVALID_ARG;
   if (n > (1L << 30) || ncols > (1L << 30)) return EVD_ERR_INVALID_ARG;
-  if (n < 3 || ncols == 0) return EVD_SUCCESS;
+  if (h0 < 0 || h0 % 8 != 0 || h1 < h0 || (h1 % 8 != 0 && h1 < n - 2)) return EVD_ERR_INVALID_ARG;
+  if (ident && (!forward || ident_k > h0)) return EVD_ERR_INVALID_ARG;
+  if (n < 3 || ncols == 0 || h0 >= n - 2 || h1 == h0) return EVD_SUCCESS;
   if (!U || !X) return EVD_ERR_INVALID_ARG;
   if (tbuf && ((uintptr_t)tbuf & 15)) return EVD_ERR_INVALID_ARG;
+  // from the identity the work of a column block grows with its index: the
+  // heaviest blocks are dispatched first
+  const Q2Range rg{(int)h0, (int)std::min(h1, n), ident ? 1 : 0, ident ? (int)ident_k : 0,
+                   ident ? 1 : 0};
   if (tbuf) {
     if (forward) {
-      EVD_TRY(launch_tbuild<true>(n, U, ldU, tbuf, st));
-      return launch_q2_pre<true>(n, ncols, U, ldU, tbuf, X, ldX, st);
+      EVD_TRY(launch_tbuild<true>(n, U, ldU, tbuf, h0, h1, st));
+      return launch_q2_pre<true>(n, ncols, U, ldU, tbuf, X, ldX, rg, st);
     }
-    EVD_TRY(launch_tbuild<false>(n, U, ldU, tbuf, st));
-    return launch_q2_pre<false>(n, ncols, U, ldU, tbuf, X, ldX, st);
+    EVD_TRY(launch_tbuild<false>(n, U, ldU, tbuf, h0, h1, st));
+    return launch_q2_pre<false>(n, ncols, U, ldU, tbuf, X, ldX, rg, st);
   }
-  return forward ? launch_q2<true, false>(n, ncols, U, ldU, nullptr, X, ldX, st)
-                 : launch_q2<false, false>(n, ncols, U, ldU, nullptr, X, ldX, st);
+  return forward ? launch_q2<true, false>(n, ncols, U, ldU, nullptr, X, ldX, rg, st)
+                 : launch_q2<false, false>(n, ncols, U, ldU, nullptr, X, ldX, rg, st);
+}
+
+int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
+             double* tbuf, cudaStream_t st) {
+  return q2_apply_range(forward, n, ncols, U, ldU, X, ldX, tbuf, 0, n, -1, st);
 }
 
 }  // namespace evd

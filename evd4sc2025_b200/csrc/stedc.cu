@@ -833,14 +833,26 @@ long stedc_ws_ints(long n) { return n <= 1 ? 8 : make_plan(n).total_i; }
 // the smaller ones stay on the batched DMMA GEMM.
 constexpr double kOzMergeMin = 64.0 * 1024 * 1024 * 1024;
 
+// Integer workspace (bytes) of the emulated merges of an order-n solve: the
+// largest merge product is (np/2) x np x (np/2) (np: the padded order).
+long stedc_oz_bytes(long n, int nmod) {
+  if (n <= 1) return 0;
+  const long np = make_plan(n).np;
+  return oz_layout(np / 2, np, np / 2 + 2, nmod, true).bytes;
+}
+
+// out_after: an event the stream waits for before Z is written (the solve
+// itself keeps its eigenvectors in its own workspace until the last kernel),
+// so that Z may alias a buffer that other streams are still reading.
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
-          long liwork, cudaStream_t st, const OzWork* oz) {
+          long liwork, cudaStream_t st, const OzWork* oz, cudaEvent_t out_after) {
   if (n < 0 || ldz < std::max(1L, n)) return EVD_ERR_INVALID_ARG;
   if (n == 0) return EVD_SUCCESS;
   if (!d || !Z || !work || !iwork || (n > 1 && !e)) return EVD_ERR_INVALID_ARG;
   if (n > (1L << 20)) return EVD_ERR_INVALID_ARG;
   if (n == 1) {
     const double one = 1.0;
+    if (out_after) EVD_CUDA_TRY(cudaStreamWaitEvent(st, out_after, 0));
     EVD_CUDA_TRY(cudaMemcpyAsync(Z, &one, sizeof(double), cudaMemcpyHostToDevice, st));
     EVD_CUDA_TRY(cudaStreamSynchronize(st));
     return EVD_SUCCESS;
@@ -1002,6 +1014,7 @@ int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long 
     EVD_LAUNCHED();
   }
   dim3 gf(ceil_div_i(n, 256), (unsigned)std::min<long>(n, 65535));
+  if (out_after) EVD_CUDA_TRY(cudaStreamWaitEvent(st, out_after, 0));
   finish_kernel<<<gf, 256, 0, st>>>(n, np, dw, Zw, np, scal, d, Z, ldz);
   EVD_LAUNCHED();
   return read_device_error(err, st);
@@ -1014,5 +1027,5 @@ extern "C" long evd_stedc_iwork_size(long n) { return evd::stedc_ws_ints(n < 0 ?
 
 extern "C" int evd_stedc(long n, double* d, double* e, double* Z, long ldz, double* work,
                          long lwork, int* iwork, long liwork, cudaStream_t stream) {
-  return evd::stedc(n, d, e, Z, ldz, work, lwork, iwork, liwork, stream, nullptr);
+  return evd::stedc(n, d, e, Z, ldz, work, lwork, iwork, liwork, stream, nullptr, nullptr);
 }

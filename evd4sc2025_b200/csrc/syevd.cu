@@ -13,6 +13,7 @@
 // multiplying by Z in a final GEMM (saves 4n^3 flops); one process can call it
 // any number of times (the reference's chasing kernel keeps a global flag that
 // makes a second call return early).
+#include <cstdlib>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -38,10 +39,17 @@ long stedc_ws_doubles(long n);
 int stebz(long n, const double* d, const double* e, double* w, double* work, cudaStream_t st);
 long stedc_ws_ints(long n);
 int stedc(long n, double* d, double* e, double* Z, long ldz, double* work, long lwork, int* iwork,
-          long liwork, cudaStream_t st, const OzWork* oz);
+          long liwork, cudaStream_t st, const OzWork* oz, cudaEvent_t out_after = nullptr);
+long stedc_oz_bytes(long n, int nmod);
 long q2_tbuf_doubles(long n);
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,
              double* tbuf, cudaStream_t st);
+int q2_apply_range(bool forward, long n, long ncols, const double* U, long ldU, double* X,
+                   long ldX, double* tbuf, long h0, long h1, long ident_k, cudaStream_t st);
+int chase_part_async(long n, long b, double* dSub, long ldSub, double* dU, long ldU, int* iwork,
+                     long s0, long s1, int part, cudaStream_t st);
+int chase_tridiag(long n, const double* dSub, long ldSub, double* d, double* e, cudaStream_t st);
+int set_identity(long m, long n, double* Q, long ldq, cudaStream_t st);
 long sbr_back_ws_doubles(long n, long b, long nk);
 int wy_merge_slabs(long n, long b, long nk, long ncolsWY, double* dW, long ldW, const double* dY,
                    long ldY, double* work, cudaStream_t st);
@@ -70,7 +78,34 @@ struct MixedOpts {
   int moduli_update;
   uint8_t* oz;
   long oz_bytes;
+  uint8_t* oz_dc;  // the divide and conquer's own integer workspace, or nullptr
+  long oz_dc_bytes;
+  uint8_t* oz_q1;  // the Q1 formation's own integer workspace, or nullptr
+  long oz_q1_bytes;
+  double* split_buf;  // an n x n buffer for the second stage-2 chain, or nullptr
 };
+
+// Orders up to this one get a separate integer workspace for the divide and
+// conquer's emulated merges (about 2.4 n^2 doubles), so that it can run while
+// the Q1 formation still uses the main one; above it (32768: 21 GB more on top
+// of about 140 GB) the divide and conquer waits for the formation instead.
+constexpr long kMixedDcOwnMax = 24576;
+// The separate regions of orders up to kMixedDcOwnMax (bytes, each 256-byte
+// aligned): the D&C's integer workspace, the Q1 formation's, and the n x n
+// buffer of the second stage-2 chain; zero sizes above it.
+struct MixedExtra {
+  long dc, q1, split, total;
+};
+MixedExtra mixed_extra(long np, long nb, int nmod) {
+  MixedExtra x{};
+  if (np > kMixedDcOwnMax) return x;
+  auto al = [](long v) { return (v + 255) / 256 * 256; };
+  x.dc = al(stedc_oz_bytes(np, nmod) + 512);
+  x.q1 = al(sbr_form_oz_bytes(np, nb, nmod) + 512);
+  x.split = al(np * np * 8);
+  x.total = x.dc + x.q1 + x.split + 256;
+  return x;
+}
 
 // integer workspace of the mixed solve for order n (padded)
 long mixed_oz_bytes(long n, long nb, int nmod, int refine_iters) {
@@ -131,7 +166,7 @@ thread_local double g_mixed[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 // has drained, also on error paths) when the call returns.
 struct SideStream {
   cudaStream_t s = nullptr;
-  cudaEvent_t ev[12] = {};
+  cudaEvent_t ev[40] = {};
   int nev = 0;
   bool timing = false;
   ~SideStream() {
@@ -141,10 +176,10 @@ struct SideStream {
     }
     for (int i = 0; i < nev; ++i) cudaEventDestroy(ev[i]);
   }
-  int init(bool timed) {
+  int init(bool timed, int prio = 0) {
     timing = timed;
-    EVD_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    for (nev = 0; nev < 12; ++nev)
+    EVD_CUDA_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
+    for (nev = 0; nev < 40; ++nev)
       EVD_CUDA_TRY(cudaEventCreateWithFlags(&ev[nev], timed ? cudaEventDefault
                                                             : cudaEventDisableTiming));
     return EVD_SUCCESS;
@@ -249,18 +284,51 @@ static int syevd_core(long n, long b, long nb, const double* A, long lda, double
 
 size_t syevd_ws_bytes(long n, long b, long nb) { return layout(n, b, nb).bytes; }
 
-// The mixed form, scheduled on two streams (the reference overlaps its host
-// divide and conquer with the back transformation in the same spirit,
-// src/EVD/myEVD.cu:503-561):
-//   main:  sy2sb (emulated trailing SYR2K) -> band pack -> chase -> D&C (Z
-//          into W) -> X = Q Z (one emulated product) -> refinement
-//   side:  after the band pack: slab merge, Q1 formed explicitly (emulated
-//          products, the lean integer GEMM beside the chase), Q1^T;
-//          after the chase: Q^T = Q2^T Q1^T (the DMMA stage-2 kernel, beside
-//          the D&C)
-// Buffers: Q1 in dA (free after the band pack), Q1^T and then Q^T in Y (free
-// after the formation), the stage-2 T factors in OA, Z in W (the main stream
-// waits for the formation before the D&C writes it).
+// Sweep ranges of the pipelined chase.  Below the split sweep k (a multiple
+// of 8): [0, 512), [512, 1536), ... doubling, the last one ending at k; from k
+// on: ranges of max(2048, (n - 2 - k) / 16) sweeps (rounded up to a multiple
+// of 8), the last one ending at sweep n - 2.  k = 0: no lower part.  Returns
+// the number of ranges r (at most 32); range i is [bounds[i], bounds[i+1]).
+static int chase_ranges(long n, long k, long bounds[34]) {
+  const long S = std::max(n - 2, 0L);
+  int c = 0;
+  bounds[c++] = 0;
+  long s = 0, len = 512;
+  while (s + len < k) {
+    s += len;
+    bounds[c++] = s;
+    len *= 2;
+  }
+  if (k > 0 && k < S) bounds[c++] = k;
+  s = std::max(k, 0L);
+  const long step = std::max(2048L, ((S - s) / 16 + 7) / 8 * 8);
+  while (s + step < S) {
+    s += step;
+    bounds[c++] = s;
+  }
+  bounds[c] = S;
+  return c;
+}
+
+// The mixed form with the stage-2 reflectors applied while the chase runs.
+// Q2^T = B A with A = the reflectors of the sweeps [0, k) and B those of the
+// sweeps [k, n - 2), each accumulated from the identity by the DMMA stage-2
+// kernel one chase range behind the chase (a CTA skips the strips that are
+// still zero below its columns).  The kernel's dependency chain (strips x
+// blocks of 8 sweeps per column) is the longest path of the solve; splitting
+// it at k = 0.39 n into two chains that run side by side about halves it
+// (A starts after the first range, B once the chase has passed k).
+//   main:   sy2sb (emulated trailing SYR2K) -> band pack -> chase, one launch
+//           per sweep range -> D&C (own integer workspace; Z into W once the
+//           Q1 formation no longer reads W)
+//   side B: slab merge, Q1 formed explicitly (emulated)
+//   side A: A = I, the ranges below k; T1 = A Q1^T; Q^T = B T1;
+//           X = Q Z (emulated, the main integer workspace)
+//   side C: B = I, the ranges from k
+// Without the extra n x n buffer (orders above kMixedDcOwnMax) there is one
+// chain, P = Q2^T in X, then Y2 = P^T Z and X = Q1 Y2.
+// Buffers: A in the extra buffer (then Q^T), B (or P) in X, Q1 in dA, T1 (or
+// Y2) in Y, Z in W, the stage-2 T factors in OA.
 static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, double* w,
                             double* X, long ldX, void* work, long lwork_bytes, int timed,
                             cudaStream_t st, const int** err_out, const MixedOpts* mx) {
@@ -279,12 +347,26 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
   int* ich = ibase + L.oIchase;
   int* ist = ibase + L.oIstedc;
   const OzWork oz{mx->nmod, mx->oz, mx->oz_bytes};
-  SideStream side;
-  EVD_TRY(side.init(timed != 0));
-  cudaStream_t sb = side.s;
-  // events: 0 start, 1 sy2sb done, 2 band packed, 3 Q1^T ready, 4 chase done,
-  // 5 Q^T ready, 6 D&C done, 7 X done, 8 refined, 9 side start of stage 2
-  cudaEvent_t* ev = side.ev;
+  const OzWork ozdc{mx->nmod, mx->oz_dc, mx->oz_dc_bytes};
+  const OzWork ozq1{mx->nmod, mx->oz_q1, mx->oz_q1_bytes};
+  const bool dc_own = mx->oz_dc != nullptr;
+  if ((size_t)q2_tbuf_doubles(n) > (size_t)n * n) return EVD_ERR_WORKSPACE;
+  double* XA = mx->split_buf;  // chain A, then Q^T
+  const bool split = XA != nullptr && n > 64;
+  const long k = split ? std::max(8L, (long)(0.39 * (double)n) / 8 * 8) : 0;
+  SideStream sideA, sideB, sideC;
+  EVD_TRY(sideA.init(timed != 0));
+  EVD_TRY(sideB.init(timed != 0));
+  EVD_TRY(sideC.init(timed != 0));
+  cudaStream_t sa = sideA.s, sb = sideB.s, sc = sideC.s;
+  // events: 0 start, 1 sy2sb done, 2 band packed, 3 Q1 ready, 4 chase done,
+  // 5 chain A (or P) done, 6 D&C done, 7 X done, 8 refined, 9 side A start,
+  // 10 chain B done, 11 products done, 12 first product done;
+  // sideB.ev[i]: chase range i done
+  cudaEvent_t* ev = sideA.ev;
+  cudaEvent_t* evr = sideB.ev;
+  long bounds[34];
+  const int nr = chase_ranges(n, k, bounds);
   if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[0], st));
   {
     NvtxRange r("evd_b200 sy2sb (emulated trailing update)");
@@ -298,46 +380,95 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
   EVD_CUDA_TRY(cudaEventRecord(ev[1], st));
   EVD_TRY(band_pack(n, b, dA, n, sub, 2 * b, st));
   EVD_CUDA_TRY(cudaEventRecord(ev[2], st));
-  // ---- side: Q1 formation beside the chase ----
+  // ---- side B: Q1 formation ----
   EVD_CUDA_TRY(cudaStreamWaitEvent(sb, ev[2], 0));
   {
     NvtxRange r("evd_b200 Q1 formation (side stream)");
     const long npcols = ((n - 1) / b) * b;
     EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, sb));
     EVD_TRY(sbr_form_q1(n, b, nb, W, n, Y, n, dA, n, SB, (size_t)sbr_back_ws_doubles(n, b, nb),
-                        sb, &oz, true));
-    EVD_TRY(oz_transpose(n, n, dA, n, Y, n, sb));  // Q1^T
+                        sb, mx->oz_q1 ? &ozq1 : &oz, true));
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[3], sb));
+  // ---- side A / side C: the chains start from the identity (OA holds the
+  // stage-2 T factors from here on) ----
+  double* PA = split ? XA : X;
+  const long ldPA = split ? n : ldX;
+  EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[2], 0));
+  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[9], sa));
+  EVD_TRY(set_identity(n, n, PA, ldPA, sa));
+  if (split) {
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sc, ev[2], 0));
+    EVD_TRY(set_identity(n, n, X, ldX, sc));
+  }
+  // ---- main: the chase, one launch per sweep range ----
   {
     NvtxRange r("evd_b200 bulge chasing");
     EVD_CUDA_TRY(cudaMemsetAsync(U, 0, sizeof(double) * n * n, st));
-    EVD_TRY(bulge_chase_async(n, b, sub, 2 * b, U, n, d, e, ich, st));
+    for (int i = 0; i < nr; ++i) {
+      EVD_TRY(chase_part_async(n, b, sub, 2 * b, U, n, ich, bounds[i], bounds[i + 1], i, st));
+      EVD_CUDA_TRY(cudaEventRecord(evr[i], st));
+    }
+    EVD_TRY(chase_tridiag(n, sub, 2 * b, d, e, st));
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[4], st));
-  // ---- side: Q^T = Q2^T Q1^T beside the D&C ----
-  EVD_CUDA_TRY(cudaStreamWaitEvent(sb, ev[4], 0));
-  if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[9], sb));
+  // ---- the chains, range by range behind the chase ----
   {
-    NvtxRange r("evd_b200 stage-2 application to Q1^T (side stream)");
-    double* tbuf = ((size_t)q2_tbuf_doubles(n) <= (size_t)n * n) ? OA : nullptr;
-    EVD_TRY(q2_apply(true, n, n, U, n, Y, n, tbuf, sb));
+    NvtxRange r("evd_b200 stage-2 reflectors beside the chase (side streams)");
+    for (int i = 0; i < nr; ++i) {
+      const bool in_b = split && bounds[i] >= k;
+      cudaStream_t s2 = in_b ? sc : sa;
+      EVD_CUDA_TRY(cudaStreamWaitEvent(s2, evr[i], 0));
+      EVD_TRY(q2_apply_range(true, n, n, U, n, in_b ? X : PA, in_b ? ldX : ldPA, OA, bounds[i],
+                             bounds[i + 1], in_b ? k : 0, s2));
+    }
   }
-  EVD_CUDA_TRY(cudaEventRecord(ev[5], sb));
-  // ---- main: D&C (Z into W once the formation no longer reads W) ----
-  EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[3], 0));
+  EVD_CUDA_TRY(cudaEventRecord(ev[5], sa));
+  EVD_CUDA_TRY(cudaEventRecord(ev[10], split ? sc : sa));
+  // ---- main: D&C; Z goes into W once the Q1 formation no longer reads W.
+  // With its own integer workspace the D&C starts right after the chase and
+  // waits for the formation only before its last kernel writes Z; otherwise
+  // it shares the formation's workspace and waits for the formation first.
+  if (!dc_own) EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[3], 0));
   {
     NvtxRange r("evd_b200 tridiagonal divide and conquer");
     EVD_TRY(stedc(n, d, e, W, n, SW, (long)stedc_ws_doubles(n), ist, (long)stedc_ws_ints(n), st,
-                  &oz));
+                  dc_own ? &ozdc : &oz, dc_own ? ev[3] : nullptr));
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[6], st));
-  EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[5], 0));
-  {
-    NvtxRange r("evd_b200 X = Q Z (emulated)");
-    EVD_TRY(oz_gemm('t', 'n', n, n, n, 1.0, Y, n, W, n, 0.0, nullptr, n, 0.0, X, ldX, mx->nmod,
-                    false, mx->oz, mx->oz_bytes, st));
+  // ---- side A: the products (emulated, the main integer workspace; the Q1
+  // formation has its own when the split buffer exists) ----
+  if (split) {
+    NvtxRange r("evd_b200 P = B A, Q^T = P Q1^T, X = Q Z (emulated, side stream)");
+    // P = B A into U (the reflectors are dead once both chains are done); B
+    // is the identity in its first k + 1 rows and columns
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[10], 0));
+    const long m = n - k - 1;
+    EVD_TRY(copy_matrix(k + 1, n, XA, n, U, n, sa));
+    EVD_TRY(oz_gemm('n', 'n', m, n, m, 1.0, X + (k + 1) + (k + 1) * ldX, ldX, XA + (k + 1), n,
+                    0.0, nullptr, n, 0.0, U + (k + 1), n, mx->nmod, false, mx->oz, mx->oz_bytes,
+                    sa));
+    if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[12], sa));
+    // Q^T = P Q1^T into the chain-A buffer
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[3], 0));
+    EVD_TRY(oz_gemm('n', 't', n, n, n, 1.0, U, n, dA, n, 0.0, nullptr, n, 0.0, XA, n, mx->nmod,
+                    false, mx->oz, mx->oz_bytes, sa));
+    // X = Q Z
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[6], 0));
+    EVD_TRY(oz_gemm('t', 'n', n, n, n, 1.0, XA, n, W, n, 0.0, nullptr, n, 0.0, X, ldX, mx->nmod,
+                    false, mx->oz, mx->oz_bytes, sa));
+  } else {
+    NvtxRange r("evd_b200 X = Q1 (P^T Z) (emulated, side stream)");
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[3], 0));
+    EVD_CUDA_TRY(cudaStreamWaitEvent(sa, ev[6], 0));
+    EVD_TRY(oz_gemm('t', 'n', n, n, n, 1.0, X, ldX, W, n, 0.0, nullptr, n, 0.0, Y, n, mx->nmod,
+                    false, mx->oz, mx->oz_bytes, sa));
+    if (timed) EVD_CUDA_TRY(cudaEventRecord(ev[12], sa));
+    EVD_TRY(oz_gemm('n', 'n', n, n, n, 1.0, dA, n, Y, n, 0.0, nullptr, n, 0.0, X, ldX, mx->nmod,
+                    false, mx->oz, mx->oz_bytes, sa));
   }
+  EVD_CUDA_TRY(cudaEventRecord(ev[11], sa));
+  EVD_CUDA_TRY(cudaStreamWaitEvent(st, ev[11], 0));
   EVD_CUDA_TRY(cudaMemcpyAsync(w, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   EVD_CUDA_TRY(cudaEventRecord(ev[7], st));
   if (mx->refine_iters > 0) {
@@ -349,20 +480,24 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
   EVD_CUDA_TRY(cudaEventRecord(ev[8], st));
   if (timed) {
     EVD_CUDA_TRY(cudaEventSynchronize(ev[8]));
-    float ms;
-    auto el = [&](int a, int z) {
+    auto el = [&](cudaEvent_t a, cudaEvent_t z) {
       float t = 0.f;
-      cudaEventElapsedTime(&t, ev[a], ev[z]);
+      // an event that this schedule did not record reads as 0 (and its
+      // error must not reach the next launch check)
+      if (cudaEventElapsedTime(&t, a, z) != cudaSuccess) {
+        (void)cudaGetLastError();
+        t = 0.f;
+      }
       return (double)t;
     };
-    g_mixed[0] = el(0, 1);
-    g_mixed[1] = el(1, 4);
-    g_mixed[2] = el(4, 6);
-    g_mixed[3] = el(2, 3);
-    g_mixed[4] = el(9, 5);
-    g_mixed[5] = el(6, 7);
-    g_mixed[6] = el(7, 8);
-    g_mixed[7] = el(0, 8);
+    g_mixed[0] = el(ev[0], ev[1]);
+    g_mixed[1] = el(ev[1], ev[4]);
+    g_mixed[2] = el(ev[4], ev[6]);
+    g_mixed[3] = el(ev[2], ev[3]);
+    g_mixed[4] = std::max(el(ev[9], ev[5]), el(ev[9], ev[10]));
+    g_mixed[5] = el(ev[6], ev[7]);
+    g_mixed[6] = el(ev[7], ev[8]);
+    g_mixed[7] = el(ev[0], ev[8]);
     g_refine_ms = g_mixed[6];
     g_timings[0] = g_mixed[0];
     g_timings[1] = g_mixed[1];
@@ -370,7 +505,6 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
     g_timings[3] = g_mixed[4];
     g_timings[4] = g_mixed[3];
     g_timings[5] = g_mixed[7];
-    (void)ms;
   }
   if (err_out) {
     *err_out = ich + n + 32;
@@ -550,7 +684,9 @@ int syevd(long n, long b, long nb, const double* A, long lda, double* w, double*
 // Mixed form: workspace = the plain solve's (any order) + the integer part.
 size_t syevd_mixed_ws_bytes(long n, long b, long nb, int nmod, int refine_iters) {
   const size_t plain = (syevd_any_ws_bytes(n, b, nb) + 255) / 256 * 256;
-  return plain + (size_t)mixed_oz_bytes(padded_order(n, nb), nb, nmod, refine_iters) + 256;
+  const long np = padded_order(n, nb);
+  return plain + (size_t)mixed_oz_bytes(np, nb, nmod, refine_iters) + 256 +
+         (size_t)mixed_extra(np, nb, nmod).total;
 }
 
 int syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, double* X,
@@ -568,8 +704,17 @@ int syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, d
   const size_t plain = (syevd_any_ws_bytes(n, b, nb) + 255) / 256 * 256;
   uint8_t* wb = reinterpret_cast<uint8_t*>(work);
   uint8_t* ozb = reinterpret_cast<uint8_t*>(((uintptr_t)(wb + plain) + 255) & ~(uintptr_t)255);
-  MixedOpts mx{nmod, refine_iters, moduli_update, ozb,
-               mixed_oz_bytes(np, nb, nmod, refine_iters)};
+  const long ozn = mixed_oz_bytes(np, nb, nmod, refine_iters);
+  const MixedExtra xt = mixed_extra(np, nb, nmod);
+  uint8_t* xb = reinterpret_cast<uint8_t*>(((uintptr_t)(ozb + ozn) + 255) & ~(uintptr_t)255);
+  MixedOpts mx{nmod, refine_iters, moduli_update, ozb, ozn, nullptr, 0, nullptr, 0, nullptr};
+  if (xt.total > 0) {
+    mx.oz_dc = xb;
+    mx.oz_dc_bytes = xt.dc;
+    mx.oz_q1 = xb + xt.dc;
+    mx.oz_q1_bytes = xt.q1;
+    mx.split_buf = reinterpret_cast<double*>(xb + xt.dc + xt.q1);
+  }
   const int* err = nullptr;
   if (!needs_pad(n, nb)) {
     EVD_TRY(syevd_mixed_core(n, b, nb, A, lda, w, X, ldX, work, (long)plain, timed, st, &err, &mx));
@@ -644,6 +789,7 @@ extern "C" int evd_syevd_mixed(long n, long b, long nb, const double* A, long ld
 }
 
 extern "C" double evd_syevd_last_refine_ms(void) { return evd::g_refine_ms; }
+
 
 extern "C" void evd_syevd_mixed_last_timings(double out_ms[8]) {
   for (int i = 0; i < 8; ++i) out_ms[i] = evd::g_mixed[i];

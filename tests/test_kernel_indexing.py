@@ -61,3 +61,98 @@ def test_right_operand_rotation_is_chunk_aligned():
             if kr >= L:
                 kr -= L
             assert kr % 8 == 0 and kr + 8 <= L
+
+
+# ---------------------------------------------------------------------------
+# Stage-2 kernel (evd4sc2025_b200/csrc/bc_back.cu): sweep ranges and the
+# identity start.  The kernel applies, per column block, strips bottom-up;
+# inside a strip the blocks of 8 sweeps of the launch's range in order, inside
+# a block the four 32-row groups bottom-up, inside a group the sweeps in order.
+# The mixed solve calls it once per chase range, starting from X = I, and a
+# CTA skips strip R when R > (first column) + (columns) + 64.
+
+import numpy as np
+
+from oracle import algos as O
+
+
+def _random_chase_u(n, seed):
+    rng = np.random.default_rng(seed)
+    U = np.zeros((n, n))
+    for s in range(n - 2):
+        for r in range(s + 1, n - 1, 32):  # the chase stores no one-row reflector
+            seg = rng.standard_normal(min(32, n - r))
+            U[r:r + len(seg), s] = seg * np.sqrt(2.0) / np.linalg.norm(seg)
+    return U
+
+
+def _kernel_order(X, U, n, ranges, cols, ident, ident_k=0):
+    X = X.copy()
+    nstrips = (n - 2 + 127) // 128
+    for h0, h1 in ranges:
+        for cb in range(0, n, cols):
+            cs = slice(cb, min(n, cb + cols))
+            for sidx in range(nstrips - 1, -1, -1):
+                R = 128 * sidx
+                H = n - 2 - R
+                nblk = (H + 7) // 8
+                bbA, bbB = h0 // 8, min(nblk, (h1 + 7) // 8)
+                if bbB <= bbA or (ident and R > cb + cols + 64 - ident_k):
+                    continue
+                for bb in range(bbA, bbB):
+                    for J in range(3, -1, -1):
+                        for p in range(8):
+                            h = 8 * bb + p
+                            if h >= H:
+                                continue
+                            r0 = R + h + 1 + 32 * J
+                            if r0 >= n:
+                                continue
+                            u = U[r0:r0 + 32, h]
+                            X[r0:r0 + 32, cs] -= np.outer(u, u @ X[r0:r0 + 32, cs])
+    return X
+
+
+def test_stage2_ranges_keep_the_generation_order():
+    n = 300
+    U = _random_chase_u(n, 5)
+    X0 = np.random.default_rng(6).standard_normal((n, 40))
+    ref = O.q2_apply(X0, U, n, 32, transpose=True)
+    for ranges in ([(0, n)], [(0, 64), (64, 200), (200, n - 2)], [(0, 8), (8, n - 2)]):
+        got = _kernel_order(X0, U, n, ranges, 40, False)
+        assert np.abs(got - ref).max() < 1e-12
+
+
+def test_stage2_identity_start_support_and_skip():
+    n = 420
+    U = _random_chase_u(n, 7)
+    X = np.eye(n)
+    # before sweep h, column c is zero below row c + 30 + h
+    for h in range(n - 2):
+        rows = np.arange(n)[:, None]
+        cols = np.arange(n)[None, :]
+        assert np.all(X[rows > cols + 30 + h] == 0.0), h
+        for r in range(h + 1, n, 32):
+            u = U[r:r + 32, h]
+            X[r:r + 32] -= np.outer(u, u @ X[r:r + 32])
+    ref = O.q2_apply(np.eye(n), U, n, 32, transpose=True)
+    assert np.abs(X - ref).max() < 1e-12
+    bounds = [0, 64, 192, n - 2]
+    for cols in (32, 64):
+        got = _kernel_order(np.eye(n), U, n, list(zip(bounds[:-1], bounds[1:])), cols, True)
+        assert np.abs(got - ref).max() < 1e-12
+
+
+def test_stage2_two_chains_from_the_identity():
+    # Q2^T = B A with A = the sweeps [0, k) and B = the sweeps [k, n-2), each
+    # applied to the identity (B skips by the shifted rule)
+    n, k = 420, 136
+    U = _random_chase_u(n, 9)
+    ref = O.q2_apply(np.eye(n), U, n, 32, transpose=True)
+    for cols in (32, 64):
+        A = _kernel_order(np.eye(n), U, n, [(0, 64), (64, k)], cols, True, 0)
+        B = _kernel_order(np.eye(n), U, n, [(k, 264), (264, n - 2)], cols, True, k)
+        assert np.abs(B @ A - ref).max() < 1e-12
+        # B is the identity in its first k + 1 rows and columns
+        assert np.array_equal(B[:k + 1, :k + 1], np.eye(k + 1))
+        assert not B[:k + 1, k + 1:].any() and not B[k + 1:, :k + 1].any()
