@@ -292,17 +292,26 @@ int evd_syevd_batched(long count, const long* n, const double* const* A, const l
 
 /* Same pipeline and outputs as evd_syevd (the reference's myEVD,
  * src/EVD/myEVD.cu:251-706), with the big contractions on the integer tensor
- * cores: the stage-1 trailing SYR2K (the reference's tc_ozimmu_syr2k,
- * api/TCblas/tc_ozimmu_syr2k.cu:631-681) and both products of every stage-1
- * back-transformation slab (myEVD.cu:135-249) are emulated products with
- * `moduli` moduli (evd_dgemm_ozaki; 14 give FP64-level operands, fewer are
- * faster and less accurate), then `refine_iters` Ogita-Aishima iterations
- * with FP64-level emulated products (the X E update with `moduli_update`,
- * <= 14) win FP64 accuracy back.  Q1 is formed explicitly (emulated
- * products) on a second stream beside the chase, Q^T = Q2^T Q1^T by the DMMA
- * stage-2 kernel beside the divide and conquer, and X = Q Z is one emulated
- * product.  The panels, the chase, the divide and conquer and the stage-2
- * reflectors are the plain FP64 kernels.
+ * cores.  These are emulated products with `moduli` moduli
+ * (evd_dgemm_ozaki; 14 give FP64-level operands, fewer are faster and less
+ * accurate):
+ *  - the stage-1 trailing SYR2K (the reference's tc_ozimmu_syr2k,
+ *    api/TCblas/tc_ozimmu_syr2k.cu:631-681);
+ *  - Q1, formed explicitly (myEVD.cu:135-249 forms it from I);
+ *  - the large divide-and-conquer merges;
+ *  - Q2^T = B A, Q^T = Q2^T Q1^T (the reference's Q, myEVD.cu:563-565) and
+ *    X = Q Z.
+ * Then `refine_iters` Ogita-Aishima iterations with FP64-level emulated
+ * products win FP64 accuracy back (the X E update uses `moduli_update`,
+ * <= 14).
+ * The chase runs as consecutive sweep ranges.  The DMMA stage-2 kernel
+ * accumulates A (the reflectors of the sweeps below 0.39 n) and B (the rest)
+ * from the identity on side streams, one range behind the chase.  The Q1
+ * formation and the divide and conquer run beside them.  Up to n = 24576
+ * the work size includes an n x n buffer and integer workspaces of their own
+ * for the divide and conquer and the Q1 formation.  The panels, the chase,
+ * the divide and conquer and the stage-2 reflectors are the plain FP64
+ * kernels.
  * refine_iters > 0 needs n <= 65535 (padded order).  work:
  * evd_syevd_mixed_work_size bytes.  Synchronises `stream`. */
 long evd_syevd_mixed_work_size(long n, long b, long nb, int moduli, int refine_iters);
@@ -313,10 +322,11 @@ int evd_syevd_mixed(long n, long b, long nb, const double* A, long lda, double* 
  * (evd_syevd_last_timings holds its other stages and, at index 5, the total) */
 double evd_syevd_last_refine_ms(void);
 /* stages (ms) of the last timed evd_syevd_mixed call on this thread: sy2sb,
- * chase, divide and conquer, Q1 formation, stage-2 application to Q1^T, X = Q Z
- * (including the wait for the side stream), refinement, total.  The mixed form
- * runs the Q1 formation and the stage-2 application on a second stream beside
- * the chase and the divide and conquer. */
+ * chase, divide and conquer (from the end of the chase), Q1 formation, the
+ * stage-2 chains (from their start to the end of the later one), the final
+ * products (from the end of the divide and conquer to X), refinement, total.
+ * The Q1 formation and the stage-2 chains run on side streams beside the
+ * chase and the divide and conquer. */
 void evd_syevd_mixed_last_timings(double out_ms[8]);
 
 /* ---- Iterative refinement of eigenpairs -------------------------------- */
