@@ -380,7 +380,7 @@ __device__ __forceinline__ void store_tile(const double (&v)[4], const TileIO& i
 // staged with the reflectors; otherwise each block's T is built here, one
 // block ahead, by the same warps.  rg restricts the kernel to a range of
 // sweeps (and marks an identity start, see Q2Range).
-template <bool FWD, bool PRE>
+template <bool FWD, bool PRE, bool RANGE>
 __global__ void __launch_bounds__(kQThreads, 2)
     q2_mma_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
                   const double* __restrict__ Tg, double* __restrict__ X, long ldX, Q2Range rg) {
@@ -401,7 +401,8 @@ __global__ void __launch_bounds__(kQThreads, 2)
   const int offU0 = seg_off(2 * t, 0) + g - 2 * t;          // Y[8i+g][2t]
   const int offU1 = seg_off(2 * t + 1, 0) + g - 2 * t - 1;  // Y[8i+g][2t+1]
 
-  const int cblk = rg.rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  // RANGE = false: every sweep, no identity start (the plain solve's launch)
+  const int cblk = (RANGE && rg.rev) ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
   const int c0 = cblk * (kQW * kQCols) + warp * kQCols;
   TileIO io;
   io.okg = c0 + g < ncols;
@@ -424,9 +425,9 @@ __global__ void __launch_bounds__(kQThreads, 2)
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;  // sweeps with reflectors in this strip
     const int nblk = (H + 7) / 8;
-    const int bbA = rg.h0 / 8, bbB = min(nblk, (rg.h1 + 7) / 8);
+    const int bbA = RANGE ? rg.h0 / 8 : 0, bbB = RANGE ? min(nblk, (rg.h1 + 7) / 8) : nblk;
     const int cnt = bbB - bbA;  // blocks of this launch's sweeps in the strip
-    if (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, kQW * kQCols)) continue;
+    if (RANGE && (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, kQW * kQCols))) continue;
     auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();  // previous strip done with Ys / Ts; zero fill visible
@@ -570,7 +571,7 @@ __device__ __forceinline__ void store_tile8(const double (&v)[2], double* cg, bo
   if (ok && r + 1 >= 0 && r + 1 < n) cg[r + 1] = v[1];
 }
 
-template <bool FWD, int NW>
+template <bool FWD, int NW, bool RANGE>
 __global__ void __launch_bounds__(NW * 32, 2)
     q2_mma8_kernel(int n, int ncols, const double* __restrict__ U, long ldU,
                    const double* __restrict__ Tg, double* __restrict__ X, long ldX, Q2Range rg) {
@@ -582,7 +583,7 @@ __global__ void __launch_bounds__(NW * 32, 2)
   const int g = lane >> 2, t = lane & 3;
   for (int e = threadIdx.x; e < kNYBuf * kYBuf; e += nthr) Ys[e] = 0.0;
   const int offW = seg_off(g, 0) + 2 * t - g;  // Y[8i+2t(+1)][g]
-  const int cblk = rg.rev ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+  const int cblk = (RANGE && rg.rev) ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
   const int c0 = cblk * (NW * kQ8Cols) + warp * kQ8Cols;
   const bool okg = c0 + g < ncols;
   double* cg = X + (long)(okg ? c0 + g : 0) * ldX;
@@ -611,9 +612,9 @@ __global__ void __launch_bounds__(NW * 32, 2)
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;
     const int nblk = (H + 7) / 8;
-    const int bbA = rg.h0 / 8, bbB = min(nblk, (rg.h1 + 7) / 8);
+    const int bbA = RANGE ? rg.h0 / 8 : 0, bbB = RANGE ? min(nblk, (rg.h1 + 7) / 8) : nblk;
     const int cnt = bbB - bbA;
-    if (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, NW * kQ8Cols)) continue;
+    if (RANGE && (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, NW * kQ8Cols))) continue;
     auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();
@@ -677,44 +678,44 @@ __global__ void __launch_bounds__(NW * 32, 2)
 
 constexpr size_t kQ8Smem = (size_t)(kNYBuf * kYBuf + kNYBuf * kVBuf) * sizeof(double);
 
-template <bool FWD, int NW>
+template <bool FWD, int NW, bool RANGE>
 int launch_q2_8(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
                 long ldX, Q2Range rg, cudaStream_t st) {
-  EVD_TRY(smem_attr_once((const void*)q2_mma8_kernel<FWD, NW>, (int)kQ8Smem));
+  EVD_TRY(smem_attr_once((const void*)q2_mma8_kernel<FWD, NW, RANGE>, (int)kQ8Smem));
   const int grid = ceil_div_i((int)ncols, NW * kQ8Cols);
-  q2_mma8_kernel<FWD, NW><<<grid, NW * 32, kQ8Smem, st>>>((int)n, (int)ncols, U, ldU, Tg, X, ldX,
-                                                          rg);
+  q2_mma8_kernel<FWD, NW, RANGE><<<grid, NW * 32, kQ8Smem, st>>>((int)n, (int)ncols, U, ldU, Tg,
+                                                                 X, ldX, rg);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
 
-template <bool FWD, bool PRE>
+template <bool FWD, bool PRE, bool RANGE>
 int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-              long ldX, Q2Range rg, cudaStream_t st);
+              long ldX, Q2Range rg, cudaStream_t st) {
+  EVD_TRY(smem_attr_once((const void*)q2_mma_kernel<FWD, PRE, RANGE>, (int)kQSmem));
+  int grid = ceil_div_i((int)ncols, kQW * kQCols);
+  q2_mma_kernel<FWD, PRE, RANGE><<<grid, kQThreads, kQSmem, st>>>((int)n, (int)ncols, U, ldU, Tg,
+                                                                  X, ldX, rg);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
 
 // With fewer 64-column CTAs than SMs (ncols < 64 x SMs: n <= 8192 on B200)
 // the 16-column kernel leaves SMs idle; the 8-column kernel (4 warps, 32
 // columns per CTA) doubles the warps (n = 4096: 19.8 -> 14.0 ms).  Above that
 // the 16-column kernel is faster (n = 16384: 436 ms against 461 ms with
 // 8-column warps, whose m8n8k4 operands double the shared-memory reads per
-// flop).
+// flop).  A launch over every sweep without an identity start takes the
+// kernels compiled without the range logic.
 template <bool FWD>
 int launch_q2_pre(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
                   long ldX, Q2Range rg, cudaStream_t st) {
+  const bool whole = !rg.ident && rg.h0 == 0 && rg.h1 >= n - 2;
   if (ncols >= 64L * device_sm_count())
-    return launch_q2<FWD, true>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
-  return launch_q2_8<FWD, 4>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
-}
-
-template <bool FWD, bool PRE>
-int launch_q2(long n, long ncols, const double* U, long ldU, const double* Tg, double* X,
-              long ldX, Q2Range rg, cudaStream_t st) {
-  EVD_TRY(smem_attr_once((const void*)q2_mma_kernel<FWD, PRE>, (int)kQSmem));
-  int grid = ceil_div_i((int)ncols, kQW * kQCols);
-  q2_mma_kernel<FWD, PRE><<<grid, kQThreads, kQSmem, st>>>((int)n, (int)ncols, U, ldU, Tg, X,
-                                                           ldX, rg);
-  EVD_LAUNCHED();
-  return EVD_SUCCESS;
+    return whole ? launch_q2<FWD, true, false>(n, ncols, U, ldU, Tg, X, ldX, rg, st)
+                 : launch_q2<FWD, true, true>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
+  return whole ? launch_q2_8<FWD, 4, false>(n, ncols, U, ldU, Tg, X, ldX, rg, st)
+               : launch_q2_8<FWD, 4, true>(n, ncols, U, ldU, Tg, X, ldX, rg, st);
 }
 
 // -V fragments of the blocks of sweeps [h0, h1) in every strip.
@@ -761,8 +762,8 @@ int q2_apply_range(bool forward, long n, long ncols, const double* U, long ldU, 
     EVD_TRY(launch_tbuild<false>(n, U, ldU, tbuf, h0, h1, st));
     return launch_q2_pre<false>(n, ncols, U, ldU, tbuf, X, ldX, rg, st);
   }
-  return forward ? launch_q2<true, false>(n, ncols, U, ldU, nullptr, X, ldX, rg, st)
-                 : launch_q2<false, false>(n, ncols, U, ldU, nullptr, X, ldX, rg, st);
+  return forward ? launch_q2<true, false, true>(n, ncols, U, ldU, nullptr, X, ldX, rg, st)
+                 : launch_q2<false, false, true>(n, ncols, U, ldU, nullptr, X, ldX, rg, st);
 }
 
 int q2_apply(bool forward, long n, long ncols, const double* U, long ldU, double* X, long ldX,

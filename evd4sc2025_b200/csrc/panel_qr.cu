@@ -106,17 +106,73 @@ __device__ __forceinline__ void warp_sum4(double (&p)[4], int lane) {
 }
 
 // Householder QR of one tile (mm <= 128 rows, 32 columns) held in registers:
-// warp w owns columns 4w..4w+3, lane l owns rows l + 32 i (i < 4).  Writes R
-// (32 x 32, upper; diag = -sign(x0) ||x||) to Rdst and leaves the reflectors in
-// the tile (column j, rows >= j; rows above hold R) for tile_form_q.  Same
-// steps as my_hou_kernel<128,32> (util/inc/kernelQR.h:215-414): u = x/||x||,
-// u0 += sign(u0), u scaled to ||u||^2 = 2.  Step j's reflector goes through
-// shared memory to every warp: one barrier per column.
+// warp w owns columns w, w + 8, w + 16, w + 24 (a[c] holds column 8c + w),
+// lane l owns rows l + 32 i (i < 4).  Writes R (32 x 32, upper; diag =
+// -sign(x0) ||x||) to Rdst and leaves the reflectors in the tile (column j,
+// rows >= j; rows above hold R) for tile_form_q.  Same steps as
+// my_hou_kernel<128,32> (util/inc/kernelQR.h:215-414): u = x/||x||,
+// u0 += sign(u0), u scaled to ||u||^2 = 2.
+// Look-ahead: once reflector j is in shared memory, the owner of column j+1
+// (another warp) applies it to that column alone, builds reflector j+1 and
+// publishes it (bar.arrive on a named barrier), and only then applies j to its
+// other columns; every other warp waits on that barrier (bar.sync) and applies
+// j to its columns.  The dependency chain per column is then one single-column
+// update and one reflector, not a reflector plus a four-column update and a
+// CTA barrier.  Barrier of column j: 1 + (j & 3) (0 is __syncthreads); at most
+// two are in flight, because a warp must wait on column j before it can
+// publish j + 1.
 struct TileSmem {
   double V[kNB * kTile];  // reflector j at V[j * kTile ..]
   double RR[kNB];
 };
 constexpr size_t kTileSmem = sizeof(TileSmem);
+
+__device__ __forceinline__ int qr_bar(int j) { return 1 + (j & 3); }
+__device__ __forceinline__ void qr_bar_arrive(int id) {
+  asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "n"(kThreads) : "memory");
+}
+__device__ __forceinline__ void qr_bar_wait(int id) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "n"(kThreads) : "memory");
+}
+
+// Reflector of column j from a[c] (c = j / 8, this warp owns j): writes
+// V[j], RR[j] and the reflector into a[c] (rows >= j).
+__device__ __forceinline__ void tile_reflector(double (&a)[4][kRPL], int j, int mm, int lane,
+                                               TileSmem& sm) {
+  const int oc = j >> 3;
+  double x[kRPL], ss = 0.0;
+#pragma unroll
+  for (int i = 0; i < kRPL; ++i) {
+    const int row = lane + 32 * i;
+    double v = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (c == oc) v = a[c][i];
+    x[i] = (row >= j && row < mm) ? v : 0.0;
+    ss = fma(x[i], x[i], ss);
+  }
+  const double nrm2 = warp_sum(ss);
+  const double x0 = __shfl_sync(0xffffffffu, x[0], j);  // row j: lane j, i = 0
+  // A zero column (nothing to annihilate) gets u = sqrt(2) e_j rather than
+  // u = 0: H = I - u u^T then only flips row j, R_jj = 0, every reflector
+  // keeps ||u||^2 = 2, and I - Q stays nonsingular for the Householder
+  // reconstruction (u = 0 would give a zero pivot there).
+  const bool live = nrm2 > 0.0;
+  const double rn = live ? rsqrt(nrm2) : 0.0;  // 1 / ||x||
+  const double u0 = x0 * rn;
+  const double u0n = live ? u0 + ((u0 >= 0.0) ? 1.0 : -1.0) : 1.4142135623730951;
+  const double s2 = live ? rsqrt(fabs(u0n)) : 1.0;
+  if (lane == 0) sm.RR[j] = live ? ((u0 >= 0.0) ? -(nrm2 * rn) : nrm2 * rn) : 0.0;
+#pragma unroll
+  for (int i = 0; i < kRPL; ++i) {
+    const int row = lane + 32 * i;
+    const double u = ((row == j) ? u0n : x[i] * rn) * s2;
+    sm.V[j * kTile + row] = u;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+      if (c == oc && row >= j) a[c][i] = u;
+  }
+}
 
 __device__ void tile_factor(double* src, long ld, int mm, double* Rdst, long ldR, TileSmem& sm) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -126,52 +182,46 @@ __device__ void tile_factor(double* src, long ld, int mm, double* Rdst, long ldR
 #pragma unroll
     for (int i = 0; i < kRPL; ++i) {
       const int row = lane + 32 * i;
-      a[c][i] = (row < mm) ? __ldcg(src + row + (long)(4 * warp + c) * ld) : 0.0;
+      a[c][i] = (row < mm) ? __ldcg(src + row + (long)(8 * c + warp) * ld) : 0.0;
     }
 
+  if (warp == 0) {
+    tile_reflector(a, 0, mm, lane, sm);
+    qr_bar_arrive(qr_bar(0));
+  }
   for (int j = 0; j < kNB; ++j) {
-    const int ow = j >> 2, oc = j & 3;
-    if (warp == ow) {
-      double x[kRPL], ss = 0.0;
-#pragma unroll
-      for (int i = 0; i < kRPL; ++i) {
-        const int row = lane + 32 * i;
-        double v = 0.0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (c == oc) v = a[c][i];
-        x[i] = (row >= j && row < mm) ? v : 0.0;
-        ss = fma(x[i], x[i], ss);
-      }
-      const double nrm2 = warp_sum(ss);
-      const double x0 = __shfl_sync(0xffffffffu, x[0], j);  // row j: lane j, i = 0
-      // A zero column (nothing to annihilate) gets u = sqrt(2) e_j rather than
-      // u = 0: H = I - u u^T then only flips row j, R_jj = 0, every reflector
-      // keeps ||u||^2 = 2, and I - Q stays nonsingular for the Householder
-      // reconstruction (u = 0 would give a zero pivot there).
-      const bool live = nrm2 > 0.0;
-      const double rn = live ? rsqrt(nrm2) : 0.0;  // 1 / ||x||
-      const double u0 = x0 * rn;
-      const double u0n = live ? u0 + ((u0 >= 0.0) ? 1.0 : -1.0) : 1.4142135623730951;
-      const double s2 = live ? rsqrt(fabs(u0n)) : 1.0;
-      if (lane == 0) sm.RR[j] = live ? ((u0 >= 0.0) ? -(nrm2 * rn) : nrm2 * rn) : 0.0;
-#pragma unroll
-      for (int i = 0; i < kRPL; ++i) {
-        const int row = lane + 32 * i;
-        const double u = ((row == j) ? u0n : x[i] * rn) * s2;
-        sm.V[j * kTile + row] = u;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (c == oc && row >= j) a[c][i] = u;
-      }
-    }
-    __syncthreads();
-    if (4 * warp + 3 <= j) continue;  // all columns of this warp factored (warp-uniform)
+    if (warp != (j & 7)) qr_bar_wait(qr_bar(j));  // reflector j is in V[j]
     double uv[kRPL];
 #pragma unroll
     for (int i = 0; i < kRPL; ++i) uv[i] = sm.V[j * kTile + lane + 32 * i];
-    // the four column dot products are reduced together; columns <= j get a
-    // zero update
+    const int j1 = j + 1;
+    const bool own1 = j1 < kNB && warp == (j1 & 7);
+    if (own1) {
+      // column j + 1 first, then its reflector, published at once
+      const int c1 = j1 >> 3;
+      double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c == c1) {
+#pragma unroll
+          for (int i = 0; i < kRPL; i += 2) {
+            p0 = fma(uv[i], a[c][i], p0);
+            p1 = fma(uv[i + 1], a[c][i + 1], p1);
+          }
+        }
+      const double dot = warp_sum(p0 + p1);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c == c1) {
+#pragma unroll
+          for (int i = 0; i < kRPL; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
+        }
+      tile_reflector(a, j1, mm, lane, sm);
+      qr_bar_arrive(qr_bar(j1));
+    }
+    if (8 * 3 + warp <= j) continue;  // all columns of this warp factored (warp-uniform)
+    // the warp's other columns right of j (column j + 1 is done above); the
+    // four dot products are reduced together
     double pc[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -186,16 +236,18 @@ __device__ void tile_factor(double* src, long ld, int mm, double* Rdst, long ldR
     warp_sum4(pc, lane);
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const double dot = (4 * warp + c > j) ? pc[c] : 0.0;
+      const int h = 8 * c + warp;
+      const double dot = (h > j && h != j1) ? pc[c] : 0.0;
 #pragma unroll
       for (int i = 0; i < kRPL; ++i) a[c][i] = fma(-dot, uv[i], a[c][i]);
     }
   }
+  __syncthreads();  // RR complete
 
-  // R: row k = lane (i = 0), column h = 4w + c; reflectors back into the tile
+  // R: row k = lane (i = 0), column h = 8c + w; reflectors back into the tile
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const int h = 4 * warp + c;
+    const int h = 8 * c + warp;
     const double r = (lane < h) ? a[c][0] : ((lane == h) ? sm.RR[h] : 0.0);
     Rdst[lane + (long)h * ldR] = r;
 #pragma unroll

@@ -156,3 +156,53 @@ def test_stage2_two_chains_from_the_identity():
         # B is the identity in its first k + 1 rows and columns
         assert np.array_equal(B[:k + 1, :k + 1], np.eye(k + 1))
         assert not B[:k + 1, k + 1:].any() and not B[k + 1:, :k + 1].any()
+
+
+# ---------------------------------------------------------------------------
+# Panel QR tile factorisation (evd4sc2025_b200/csrc/panel_qr.cu, tile_factor):
+# warp w owns columns w, w + 8, ...; the owner of column j + 1 publishes
+# reflector j + 1 with bar.arrive on barrier 1 + ((j + 1) & 3), every other
+# warp waits on barrier 1 + (j & 3) before applying reflector j.  A barrier
+# instance completes once all 8 warps have arrived (arrive or sync).
+
+def _qr_barrier_program(w, nw=8, nb=32):
+    ops = [("arrive", 0)] if w == 0 else []
+    for j in range(nb):
+        if w != (j & 7):
+            ops.append(("sync", j))
+        if j + 1 < nb and w == ((j + 1) & 7):
+            ops.append(("arrive", j + 1))
+    return ops
+
+
+def test_panel_qr_barrier_protocol_cannot_deadlock():
+    import random
+    nw = 8
+    progs = [_qr_barrier_program(w) for w in range(nw)]
+    # every column's barrier gets exactly one arrival per warp
+    for j in range(32):
+        assert sorted(w for w in range(nw) for op in progs[w] if op[1] == j) == list(range(nw))
+    rng = random.Random(3)
+    for _ in range(3000):
+        pc, arrived, current, waiting = [0] * nw, {}, {}, [None] * nw
+        while True:
+            for w in range(nw):
+                if waiting[w] is not None and len(arrived.get(waiting[w], ())) == nw:
+                    waiting[w] = None
+                    pc[w] += 1
+            run = [w for w in range(nw) if pc[w] < len(progs[w]) and waiting[w] is None]
+            if not run:
+                assert all(pc[w] == len(progs[w]) for w in range(nw)), "deadlock"
+                break
+            w = rng.choice(run)
+            op, j = progs[w][pc[w]]
+            bid = 1 + (j & 3)
+            open_j = current.get(bid)
+            # a barrier id is reused only after its previous instance completed
+            assert open_j is None or open_j == j or len(arrived[open_j]) == nw
+            current[bid] = j
+            arrived.setdefault(j, set()).add(w)
+            if op == "arrive":
+                pc[w] += 1
+            else:
+                waiting[w] = j
