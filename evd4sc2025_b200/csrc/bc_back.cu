@@ -247,9 +247,16 @@ struct Q2Range {
   int rev;  // CTA b takes column block gridDim.x - 1 - b (the heaviest first)
 };
 
-__host__ __device__ __forceinline__ bool q2_skip_strip(const Q2Range& rg, long R, long cta_col0,
-                                                       int cta_cols) {
-  return rg.ident && R > cta_col0 + cta_cols + 64 - rg.ident_k;
+// Strips 0 .. q2_strips() - 1 are the ones a CTA processes: those with a
+// block of the range's sweeps (R < n - 2 - h0) and, from the identity, not
+// wholly below the CTA's columns (R <= first column + columns + 64 - k).
+// Both conditions bound R from above, so the strips form a prefix.
+__host__ __device__ __forceinline__ int q2_strips(const Q2Range& rg, int n, int nstrips,
+                                                  long cta_col0, int cta_cols) {
+  long rmax = (long)n - 3 - rg.h0;
+  if (rg.ident) rmax = min(rmax, cta_col0 + cta_cols + 64 - (long)rg.ident_k);
+  if (rmax < 0) return 0;
+  return (int)min((long)nstrips, rmax / kStrip + 1);
 }
 
 // -V fragments of every block of every strip (one CTA per block, one warp
@@ -420,14 +427,14 @@ __global__ void __launch_bounds__(kQThreads, 2)
     for (int e = threadIdx.x; e < kVBuf / 2; e += kQThreads) cp_async16(dst + 2 * e, src + 2 * e);
   };
   const long cta_col0 = (long)cblk * (kQW * kQCols);
-  for (int si = 0; si < nstrips; ++si) {
-    const int sidx = FWD ? (nstrips - 1 - si) : si;
+  const int ns = RANGE ? q2_strips(rg, n, nstrips, cta_col0, kQW * kQCols) : nstrips;
+  for (int si = 0; si < ns; ++si) {
+    const int sidx = FWD ? (ns - 1 - si) : si;
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;  // sweeps with reflectors in this strip
     const int nblk = (H + 7) / 8;
     const int bbA = RANGE ? rg.h0 / 8 : 0, bbB = RANGE ? min(nblk, (rg.h1 + 7) / 8) : nblk;
-    const int cnt = bbB - bbA;  // blocks of this launch's sweeps in the strip
-    if (RANGE && (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, kQW * kQCols))) continue;
+    const int cnt = bbB - bbA;  // blocks of this launch's sweeps in the strip (>= 1)
     auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();  // previous strip done with Ys / Ts; zero fill visible
@@ -607,14 +614,14 @@ __global__ void __launch_bounds__(NW * 32, 2)
     for (int e = threadIdx.x; e < kVBuf / 2; e += nthr) cp_async16(dst + 2 * e, src + 2 * e);
   };
   const long cta_col0 = (long)cblk * (NW * kQ8Cols);
-  for (int si = 0; si < nstrips; ++si) {
-    const int sidx = FWD ? (nstrips - 1 - si) : si;
+  const int ns = RANGE ? q2_strips(rg, n, nstrips, cta_col0, NW * kQ8Cols) : nstrips;
+  for (int si = 0; si < ns; ++si) {
+    const int sidx = FWD ? (ns - 1 - si) : si;
     const long R = (long)sidx * kStrip;
     const int H = n - 2 - (int)R;
     const int nblk = (H + 7) / 8;
     const int bbA = RANGE ? rg.h0 / 8 : 0, bbB = RANGE ? min(nblk, (rg.h1 + 7) / 8) : nblk;
     const int cnt = bbB - bbA;
-    if (RANGE && (cnt <= 0 || q2_skip_strip(rg, R, cta_col0, NW * kQ8Cols))) continue;
     auto bb_of = [&](int it) { return FWD ? (bbA + it) : (bbB - 1 - it); };
 
     __syncthreads();

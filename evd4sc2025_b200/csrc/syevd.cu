@@ -386,8 +386,10 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
     NvtxRange r("evd_b200 Q1 formation (side stream)");
     const long npcols = ((n - 1) / b) * b;
     EVD_TRY(wy_merge_slabs(n, b, nb, npcols, W, n, Y, n, SB, sb));
+    // the 4-stage integer GEMM beside the two chains (measured faster there);
+    // the 2-stage one beside the single chain, whose CTAs it shares SMs with
     EVD_TRY(sbr_form_q1(n, b, nb, W, n, Y, n, dA, n, SB, (size_t)sbr_back_ws_doubles(n, b, nb),
-                        sb, mx->oz_q1 ? &ozq1 : &oz, true));
+                        sb, mx->oz_q1 ? &ozq1 : &oz, /*lean=*/!split));
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[3], sb));
   // ---- side A / side C: the chains start from the identity (OA holds the
