@@ -8,12 +8,12 @@
 //
 // * tc_syr2k and the half SYR2K run one tcgen05 kernel: both operands are
 //   packed once as FP16 rows with K contiguous (into the reference's `hwork`
-//   when it fits, else a stream-ordered buffer), streamed into 128-byte-
-//   swizzled shared-memory tiles by copy warps, multiplied 64 K at a time by
-//   `tcgen05.mma.kind::f16` into a 128 x 128 FP32 accumulator in tensor
-//   memory, and the epilogue applies alpha / beta on the lower triangle.
-//   A B^T + B A^T is one product over the concatenated K range:
-//   [A | B] * [B | A]^T.
+//   when it fits, else a stream-ordered buffer), copied by TMA into 128-byte-
+//   swizzled shared-memory tiles, multiplied 64 K at a time by
+//   `tcgen05.mma.kind::f16` (M128 N256) into FP32 accumulators in tensor
+//   memory by a persistent warp-specialised kernel, and the epilogue applies
+//   alpha / beta on the lower triangle.  A B^T + B A^T is one product over
+//   the concatenated K range: [A | B] * [B | A]^T.
 // * the FP32 SYR2K is a SIMT FP32 kernel (exact FP32 multiply-add, the
 //   arithmetic of CUBLAS_COMPUTE_32F that the reference asks cuBLAS for).
 // * the FP32 / FP16 panel QR and TSQR convert the panel to FP64, run the
@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "ozaki.cuh"
 #include "panel_qr.cuh"
 
 namespace evd {
@@ -202,10 +203,10 @@ __global__ void __launch_bounds__(256) ssyr2k_kernel(long n, long k, float alpha
 }
 
 // ------------------------------------------------ tcgen05 FP16 SYR2K (TMEM)
-// Tile 128 x 128 of C per CTA; the operands are packed once into FP16 rows
-// with K contiguous (below), then streamed into shared memory and multiplied
-// by tcgen05.mma into an FP32 accumulator in tensor memory.
-constexpr int kTM = 128, kTN = 128;
+// The operands are packed once into FP16 rows with K contiguous (below), then
+// copied into shared memory by TMA and multiplied by tcgen05.mma into FP32
+// accumulators in tensor memory.
+constexpr int kTM = 128;  // rows of a tile of C (grid-size check)
 constexpr unsigned long long kTWaitNs = 2000000000ull;  // 2 s per wait: far above any chunk
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -249,19 +250,6 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
 }
 
 
-// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B F16 (0),
-// both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(kTN >> 3) << 17) | ((uint32_t)(kTM >> 4) << 24);
-
-__device__ __forceinline__ void umma_f16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
-      : "memory");
-}
-
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
@@ -271,6 +259,11 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __device__ __forceinline__ float ld_elem(const float* p) { return __ldg(p); }
 __device__ __forceinline__ float ld_elem(const __half* p) { return __half2float(p[0]); }
 
+__device__ __forceinline__ float ld_c(const float* c) { return *c; }
+__device__ __forceinline__ float ld_c(const __half* c) { return __half2float(*c); }
+__device__ __forceinline__ void st_c(float* c, float v) { *c = v; }
+__device__ __forceinline__ void st_c(__half* c, float v) { *c = __float2half_rn(v); }
+
 __device__ __forceinline__ void store_c(float* c, float v, float alpha, float beta) {
   *c = (beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * *c);
 }
@@ -278,20 +271,10 @@ __device__ __forceinline__ void store_c(__half* c, float v, float alpha, float b
   *c = __float2half_rn((beta == 0.0f) ? alpha * v : fmaf(alpha, v, beta * __half2float(*c)));
 }
 
-// ---- FP16 operand copy + cp.async-fed tensor-core SYR2K ----
-// H (n rows x L = 2 k8 halves, K contiguous per row, k8 = k rounded up to 8):
-// H[m][kk] = A(m, kk), H[m][k8 + kk] = B(m, kk), zero in the padding.  Rows of
-// H are the K-major rows the tensor core reads, so a stage is filled by
-// 16-byte cp.async copies straight into the core-matrix layout.
-// 16-byte copy through L1 (.ca): two threads share each 32-byte sector, and
-// the L1-allocating form moved about 13 % more operand bytes per second than
-// .cg in the tensor-core kernel below.
-__device__ __forceinline__ void cp_async16z(void* smem, const void* gmem, int src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)),
-               "l"(gmem), "r"(src_bytes)
-               : "memory");
-}
-
+// ---- FP16 operand copy + TMA-fed tensor-core SYR2K ----
+// H (n rows x L = 2 kp halves, K contiguous per row, kp = k rounded up to
+// 64): H[m][kk] = A(m, kk), H[m][kp + kk] = B(m, kk), zero in the padding.
+// Rows of H are the K-major rows the tensor core reads.
 template <typename TI>
 __global__ void pack_h_kernel(long n, long k, long k8, const TI* __restrict__ A, long lda,
                               const TI* __restrict__ B, long ldb, __half* __restrict__ H) {
@@ -317,30 +300,32 @@ __global__ void pack_h_kernel(long n, long k, long k8, const TI* __restrict__ A,
   }
 }
 
-// The tensor-core kernel for packed operands: warps 0-3 copy (16-byte
-// cp.async, K chunks of 64 through 3 stages, 2 chunks in flight per thread),
-// warp 4 issues the MMAs.  Operand tiles use the 128-byte-swizzled K-major
-// layout: row r of a tile is 128 contiguous bytes (64 halves of K) at
-// (r / 8) * 1024 + (r % 8) * 128, its 16-byte chunk c stored at chunk
-// c ^ (r % 8), tiles 1024-byte aligned; the descriptor says SWIZZLE_128B with
-// a 1024-byte stride between 8-row groups, and the K16 steps inside a chunk
-// advance the start address by 32 bytes.  A producer completes its own copies
-// of a chunk (wait_group), makes them visible to the tensor core
-// (fence.proxy.async) and arrives on the chunk's `full` barrier (128
-// arrivals); the MMA warp waits on `full`, issues four K16 MMAs and commits
-// them to the stage's `empty` barrier, which the producers wait on before
-// refilling the stage.  No block-wide barrier in the main loop; every wait is
-// bounded.
-constexpr int kWK = 64, kWS = 3, kWD = kWS - 1;      // K chunk, stages, chunks in flight
-constexpr int kWTile = kTM * kWK * 2;                // 16 KB per operand tile
-constexpr int kWStage = 2 * kWTile;
-constexpr int kWProd = 128, kWThreads = kWProd + 32;
-constexpr int kWSmem = kWS * kWStage + 1024 + 256;   // + alignment slack, barriers
+// The tensor-core kernel for packed operands: persistent and warp-
+// specialised, one CTA per SM walking the lower 128 x 256 tiles of C
+// (t = blockIdx.x, + gridDim.x, ...).  Warp 0 lane 0 issues TMA copies
+// (cp.async.bulk.tensor, 128-byte swizzle, this GPU's own memory, no
+// multicast) of 64-wide K chunks of [A | B] (128 rows) and [B | A] (256 rows)
+// into a 4-stage ring; warp 1 lane 0 issues four tcgen05.mma.kind::f16
+// M128 N256 K16 per chunk into one of two 256-column FP32 accumulators in
+// tensor memory (tile i into buffer i & 1); warps 2-5 drain the other buffer
+// (tcgen05.ld, alpha / beta, lower triangle only) while the next tile is
+// multiplied.  Every wait is bounded; the MMA thread waits for its last MMAs
+// before the tensor memory is freed.  The packed rows are K-major with the K
+// range padded to a multiple of 64, so the [B | A] chunk of K offset
+// 64 t + kp (mod 2 kp) is one box.
+constexpr int kGM = 128, kGN = 256, kGK = 64;        // tile rows, columns, K per chunk
+constexpr uint32_t kGTileA = kGM * kGK * 2;          // 16 KB
+constexpr uint32_t kGTileB = kGN * kGK * 2;          // 32 KB
+constexpr uint32_t kGStage = kGTileA + kGTileB;      // 48 KB
+constexpr int kGStages = 4;
+constexpr int kGThreads = 192;
+constexpr int kGSmem = kGStages * (int)kGStage + 1024 + 256;
+// kind::f16 instruction descriptor for M128 N256: D F32, A and B F16, K-major
+constexpr uint32_t kGIdesc = (1u << 4) | ((uint32_t)(kGN >> 3) << 17) | ((uint32_t)(kGM >> 4) << 24);
 
 __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
-  // start >> 4 | LBO 16 B (unused for swizzled K-major) | SBO 1024 B | version 1 |
-  // base offset 0 (tiles 1024-aligned, K steps stay inside a 128-byte row) |
-  // layout SWIZZLE_128B (2)
+  // start >> 4 | LBO 16 B (unused for swizzled K-major) | SBO 1024 B (8-row
+  // groups) | version 1 | base offset 0 (tiles 1024-aligned) | SWIZZLE_128B
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          (1ull << 46) | (2ull << 61);
 }
@@ -349,38 +334,75 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tma_load2(void* dst, const CUtensorMap* map, int x, int y,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void umma_f16_n256(uint32_t tmem, uint64_t da, uint64_t db,
+                                              uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(kGIdesc), "r"(acc)
+      : "memory");
+}
+
+// lower tile t (column block bn holds the 128-row tile rows 2 bn .. tm - 1)
+__device__ __forceinline__ void g_tile(long t, int tm, int& bm, int& bn) {
+  int c = 0;
+  for (;; ++c) {
+    const long cnt = tm - 2L * c;
+    if (t < cnt) break;
+    t -= cnt;
+  }
+  bn = c;
+  bm = 2 * c + (int)t;
+}
 
 template <typename TC>
-__global__ void __launch_bounds__(kWThreads) tc_syr2k_ws_kernel(long n, long k8, float alpha,
-                                                                const __half* __restrict__ H,
-                                                                float beta, TC* __restrict__ C,
-                                                                long ldc, int* err) {
-  extern __shared__ __align__(1024) uint8_t tsm[];
-  // 1024-byte aligned tile area (the swizzle pattern repeats every 1024 bytes)
-  uint8_t* stages = tsm + ((1024u - (smem_u32(tsm) & 1023u)) & 1023u);
-  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kWS * kWStage);
-  uint64_t* empty = full + kWS;
-  uint64_t* done = empty + kWS;
+__global__ void __launch_bounds__(kGThreads, 1)
+    tc_syr2k_tma_kernel(const __grid_constant__ CUtensorMap mapL,
+                        const __grid_constant__ CUtensorMap mapR, long n, long kp, float alpha,
+                        float beta, TC* __restrict__ C, long ldc, int tm, long ntiles, int* err) {
+  extern __shared__ __align__(1024) uint8_t gsm[];
+  uint8_t* stages = gsm + ((1024u - (smem_u32(gsm) & 1023u)) & 1023u);
+  uint64_t* full = reinterpret_cast<uint64_t*>(stages + kGStages * kGStage);
+  uint64_t* empty = full + kGStages;
+  uint64_t* tfull = empty + kGStages;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* done = tempty + 2;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-  long bi, bj;
-  tri_tile(blockIdx.x, bi, bj);
-  const long m0 = bi * kTM, n0 = bj * kTN;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long L = 2 * k8;
-  const long nch = (L + kWK - 1) / kWK;
+  const long L = 2 * kp;
+  const long nk = L / kGK;
 
   if (tid == 0) {
-    for (int s = 0; s < kWS; ++s) {
-      mbar_init(full + s, kWProd);
+    for (int s = 0; s < kGStages; ++s) {
+      mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(tfull + b, 1);
+      mbar_init(tempty + b, 128);
     }
     mbar_init(done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapL)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapR)) : "memory");
   }
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(tslot)),
-                 "r"(kTN)
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     smem_u32(tslot))
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -389,117 +411,136 @@ __global__ void __launch_bounds__(kWThreads) tc_syr2k_ws_kernel(long n, long k8,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tslot;
 
-  bool ok = true;
-  if (warp < 4) {
-    // ---- producers: chunk t -> stage t % kWS ----
-    auto issue = [&](long t, int s) {
-      uint8_t* Lt = stages + s * kWStage;
-      uint8_t* Rt = Lt + kWTile;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int q = tid + i * kWProd;
-        const int row = q >> 3, c = q & 7;  // 8 threads per 128-byte row: coalesced
-        const int off = (row >> 3) * 1024 + (row & 7) * 128 + ((c ^ (row & 7)) << 4);
-        const long kk = t * kWK + c * 8;
-        const bool kv = kk < L;
-        long kr = kk + k8;
-        if (kr >= L) kr -= L;
-        const long gl = m0 + row, gr = n0 + row;
-        const bool lv = kv && gl < n, rv = kv && gr < n;
-        cp_async16z(Lt + off, lv ? (const void*)(H + gl * L + kk) : (const void*)H, lv ? 16 : 0);
-        cp_async16z(Rt + off, rv ? (const void*)(H + gr * L + kr) : (const void*)H, rv ? 16 : 0);
-      }
-    };
-    long arrived = 0;  // chunks whose `full` barrier this thread has arrived on
-    for (long t = 0; t < nch; ++t) {
-      const int s = (int)(t % kWS);
-      if (t >= kWS && !mbar_wait(empty + s, (uint32_t)((t / kWS - 1) & 1), err)) {
-        ok = false;
-        break;
-      }
-      issue(t, s);
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      if (t >= kWD - 1) {  // chunk t - (kWD - 1) has landed
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kWD - 1) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(full + (int)(arrived % kWS));
-        ++arrived;
-      }
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (ok)
-      for (; arrived < nch; ++arrived) mbar_arrive(full + (int)(arrived % kWS));
-  } else {
-    // ---- MMA warp: lane 0 issues, the whole warp waits ----
-    for (long t = 0; t < nch; ++t) {
-      const int s = (int)(t % kWS);
-      if (!mbar_wait(full + s, (uint32_t)((t / kWS) & 1), err)) {
-        ok = false;
-        break;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t la = smem_u32(stages + s * kWStage), ra = la + kWTile;
-#pragma unroll
-        for (int ks = 0; ks < kWK / 16; ++ks)
-          umma_f16(tmem, smem_desc_sw128(la + ks * 32), smem_desc_sw128(ra + ks * 32),
-                   (t > 0 || ks > 0) ? 1u : 0u);
-        umma_commit(empty + s);
-      }
-      __syncwarp();
-    }
-    if (lane == 0) umma_commit(done);  // all MMAs issued above complete -> done
-    __syncwarp();
-  }
-  const bool fin = mbar_wait(done, 0, err);
-  ok = __syncthreads_and(ok && fin);
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok && warp < 4) {
-    const long gi = m0 + warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < kTN; c0 += 16) {
-      uint32_t v[16];
-      const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-          "%11, %12, %13, %14, %15}, [%16];"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-            "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-          : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (gi < n) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const long gj = n0 + c0 + j;
-          if (gj <= gi) store_c(C + gi + gj * ldc, __uint_as_float(v[j]), alpha, beta);
+  if (warp == 0) {
+    if (lane == 0) {  // ---- TMA producer ----
+      long gk = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        int bm, bn;
+        g_tile(t, tm, bm, bn);
+        for (long kb = 0; kb < nk; ++kb, ++gk) {
+          const int s = (int)(gk % kGStages);
+          if (gk >= kGStages &&
+              !mbar_wait(empty + s, (uint32_t)((gk / kGStages - 1) & 1), err)) {
+            ok = false;
+            break;
+          }
+          uint8_t* sa = stages + s * kGStage;
+          long kr = kb * kGK + kp;
+          if (kr >= L) kr -= L;
+          mbar_expect_tx(full + s, kGStage);
+          tma_load2(sa, &mapL, (int)(kb * kGK), bm * kGM, full + s);
+          tma_load2(sa + kGTileA, &mapR, (int)kr, bn * kGN, full + s);
         }
       }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // ---- MMA issuer ----
+      long gk = 0;
+      int i = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+        const int b = i & 1;
+        if (i >= 2 && !mbar_wait(tempty + b, (uint32_t)(((i >> 1) - 1) & 1), err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc_tm = tmem + (uint32_t)(b * kGN);
+        for (long kb = 0; kb < nk; ++kb, ++gk) {
+          const int s = (int)(gk % kGStages);
+          if (!mbar_wait(full + s, (uint32_t)((gk / kGStages) & 1), err)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t sa = smem_u32(stages + s * kGStage);
+          const uint32_t sb = sa + kGTileA;
+#pragma unroll
+          for (int ks = 0; ks < kGK / 16; ++ks)
+            umma_f16_n256(acc_tm, smem_desc_sw128(sa + ks * 32), smem_desc_sw128(sb + ks * 32),
+                          (kb > 0 || ks > 0) ? 1u : 0u);
+          umma_commit(empty + s);
+        }
+        if (ok) umma_commit(tfull + b);
+      }
+      umma_commit(done);  // fires when every MMA issued above has completed
+      mbar_wait(done, 0, err);
+    }
+  } else {  // ---- epilogue: warps 2-5, TMEM lanes 32 (warp % 4) .. + 31 ----
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    int i = 0;
+    for (long t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      if (!mbar_wait(tfull + b, (uint32_t)((i >> 1) & 1), err)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      int bm, bn;
+      g_tile(t, tm, bm, bn);
+      const long gi = (long)bm * kGM + row;
+      const long n0 = (long)bn * kGN;
+#pragma unroll 1
+      for (int c0 = 0; c0 < kGN; c0 += 32) {
+        uint32_t v[32];
+        const uint32_t addr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kGN + c0);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+              "%10, %11, %12, %13, %14, %15}, [%16];"
+              : "=r"(v[16 * h + 0]), "=r"(v[16 * h + 1]), "=r"(v[16 * h + 2]),
+                "=r"(v[16 * h + 3]), "=r"(v[16 * h + 4]), "=r"(v[16 * h + 5]),
+                "=r"(v[16 * h + 6]), "=r"(v[16 * h + 7]), "=r"(v[16 * h + 8]),
+                "=r"(v[16 * h + 9]), "=r"(v[16 * h + 10]), "=r"(v[16 * h + 11]),
+                "=r"(v[16 * h + 12]), "=r"(v[16 * h + 13]), "=r"(v[16 * h + 14]),
+                "=r"(v[16 * h + 15])
+              : "r"(addr + 16 * h));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (gi < n) {
+          const long j0 = n0 + c0;
+          // columns j0 .. min(j0 + 31, gi, n - 1) of row gi (jl + 1 of them);
+          // the reads of C are issued together before any store (the compiler
+          // cannot tell that the stores do not alias them, so it would
+          // otherwise wait for each read in turn); every index is static, so
+          // v and cv stay in registers
+          const long jl = (gi < n - 1 ? gi : n - 1) - j0;
+          TC* c = C + gi + j0 * ldc;
+          float cv[32];
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = (beta != 0.0f && j <= jl) ? ld_c(c + j * ldc) : 0.0f;
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (j <= jl) st_c(c + j * ldc, fmaf(beta, cv[j], alpha * __uint_as_float(v[j])));
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(tempty + b);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTN)
-                 : "memory");
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
 }
 
-// A, B -> H in `hwork` (n x 2 k8 halves), then the warp-specialised kernel.
+// A, B -> H (n rows x 2 kp halves, kp = k rounded up to 64), then the
+// persistent kernel.
 template <typename TI, typename TC>
 int tc_syr2k_packed(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
                     float beta, TC* C, long ldc, __half* H, int* err, cudaStream_t st) {
-  const long k8 = (k + 7) / 8 * 8;
-  const long L = 2 * k8;
+  const long kp = (k + 63) / 64 * 64;
+  const long L = 2 * kp;
   dim3 pg((unsigned)((n + 31) / 32), (unsigned)((L + 31) / 32));
-  pack_h_kernel<TI><<<pg, dim3(32, 8), 0, st>>>(n, k, k8, A, lda, B, ldb, H);
+  pack_h_kernel<TI><<<pg, dim3(32, 8), 0, st>>>(n, k, kp, A, lda, B, ldb, H);
   EVD_LAUNCHED();
-  const long T = (n + kTM - 1) / kTM;
-  EVD_CUDA_TRY(cudaFuncSetAttribute(tc_syr2k_ws_kernel<TC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, kWSmem));
-  tc_syr2k_ws_kernel<TC><<<(unsigned)(T * (T + 1) / 2), kWThreads, kWSmem, st>>>(
-      n, k8, alpha, H, beta, C, ldc, err);
+  CUtensorMap mapL, mapR;
+  EVD_TRY(tma_map_rows16(&mapL, H, n, L, L, kGM));
+  EVD_TRY(tma_map_rows16(&mapR, H, n, L, L, kGN));
+  const int tm = (int)((n + kGM - 1) / kGM);
+  long ntiles = 0;
+  for (long c = 0; 2 * c < tm; ++c) ntiles += tm - 2 * c;
+  const int grid = (int)std::min<long>(ntiles, device_sm_count());
+  EVD_TRY(smem_attr_once((const void*)tc_syr2k_tma_kernel<TC>, kGSmem));
+  tc_syr2k_tma_kernel<TC><<<grid, kGThreads, kGSmem, st>>>(mapL, mapR, n, kp, alpha, beta, C, ldc,
+                                                           tm, ntiles, err);
   EVD_LAUNCHED();
   return EVD_SUCCESS;
 }
@@ -588,7 +629,7 @@ cudaMemPool_t lp_pool() {
 template <typename TI, typename TC>
 int tc_syr2k_run(long n, long k, float alpha, const TI* A, long lda, const TI* B, long ldb,
                  float beta, TC* C, long ldc, __half* H, cudaStream_t st) {
-  const long k8 = (k + 7) / 8 * 8;
+  const long k8 = (k + 63) / 64 * 64;  // the packed K range (a multiple of 64)
   if ((2 * k8 + 31) / 32 >= 65536 || (n + 31) / 32 >= (1L << 31)) return EVD_ERR_INVALID_ARG;
   int* err = tc_err_word();
   if (!err) return EVD_ERR_CUDA;
@@ -661,8 +702,8 @@ extern "C" int evd_tc_syr2k(long n, long k, float alpha, const float* A, long ld
   if (n == 0) return EVD_SUCCESS;
   if (k == 0 || alpha == 0.0f) return evd::scale_lower(n, beta, C, ldc, stream);
   // the reference's FP16 workspace (2 n k halves) holds the packed operands
-  // when k % 8 == 0; otherwise (or without one) a stream-ordered buffer does
-  const bool own = hwork == nullptr || k % 8 != 0 || ((uintptr_t)hwork & 15) != 0;
+  // when k % 64 == 0; otherwise (or without one) a stream-ordered buffer does
+  const bool own = hwork == nullptr || k % 64 != 0 || ((uintptr_t)hwork & 15) != 0;
   return evd::tc_syr2k_run(n, k, alpha, A, lda, B, ldb, beta, C, ldc,
                            own ? nullptr : (__half*)hwork, stream);
 }

@@ -674,6 +674,24 @@ int make_plane_map(CUtensorMap* map, const int8_t* base, long rows, long K, long
   return r == CUDA_SUCCESS ? EVD_SUCCESS : EVD_ERR_CUDA;
 }
 
+}  // namespace
+
+int tma_map_rows16(CUtensorMap* map, const void* base, long rows, long elems, long ld,
+                   int box_rows) {
+  auto enc = encode_fn();
+  if (!enc) return EVD_ERR_CUDA;
+  cuuint64_t dims[2] = {(cuuint64_t)elems, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {64u, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(base), dims,
+                   strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? EVD_SUCCESS : EVD_ERR_CUDA;
+}
+
+namespace {
+
 int* oz_err_word() {
   static int* words[64] = {nullptr};
   static std::mutex mu;

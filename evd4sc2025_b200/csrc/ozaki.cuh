@@ -2,6 +2,7 @@
 // kernels and their description are in ozaki.cu.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,6 +19,11 @@ struct OzLayout {
 };
 
 long oz_ld(long K);  // row pitch (bytes) of a quantised operand: K rounded up to 128
+// 2-D tiled tensor map over `rows` rows of 16-bit elements (`elems` used of
+// a row pitch of `ld` elements): boxes of 64 elements (128 bytes) x box_rows,
+// 128-byte swizzle, zero fill outside the tensor.
+int tma_map_rows16(CUtensorMap* map, const void* base, long rows, long elems, long ld,
+                   int box_rows);
 OzLayout oz_layout(long M, long N, long K, int nmod, bool need_transpose);
 // bits P of the integer operands for nmod moduli and inner dimension K
 int oz_bits(int nmod, long K);

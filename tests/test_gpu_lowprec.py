@@ -53,7 +53,7 @@ def _check_lower(Cout, C0, ref, bound, k, extra_rel=0.0):
 @pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (0.5, 0.0), (2.0, -0.25)])
 @pytest.mark.parametrize("packed", [True, False])
 def test_tc_syr2k(cuda, evdlib, n, k, alpha, beta, packed):
-    """packed: operands packed into the caller's FP16 workspace (k % 8 == 0;
+    """packed: operands packed into the caller's FP16 workspace (k % 64 == 0;
     other k use the library's buffer); else into the library's buffer."""
     A, B, Cm = _data(n, k, n * 7 + k, cuda)
     if beta == 0.0:
