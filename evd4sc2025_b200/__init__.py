@@ -418,14 +418,19 @@ myEVD = syevd
 
 
 class MixedWorkspace:
-    """Reusable device workspace for :func:`syevd_mixed`."""
+    """Reusable device workspace for :func:`syevd_mixed`.  ``minimal``: the
+    smallest workspace the solve accepts (one stage-2 chain, the divide and
+    conquer after the Q1 formation: slower, about 3.4 n^2 doubles less)."""
 
     def __init__(self, n: int, b: int = 32, nb: int = 1024, moduli: int = 14,
-                 refine_iters: int = 0, device="cuda"):
-        nbytes = lib().evd_syevd_mixed_work_size(n, b, nb, moduli, refine_iters)
+                 refine_iters: int = 0, device="cuda", minimal: bool = False):
+        size_fn = (lib().evd_syevd_mixed_work_size_min if minimal
+                   else lib().evd_syevd_mixed_work_size)
+        nbytes = size_fn(n, b, nb, moduli, refine_iters)
         if nbytes <= 0:
             raise EvdError("evd_syevd_mixed_work_size", -1)
         self.key = (n, b, nb, moduli, refine_iters)
+        self.minimal = minimal
         self.nbytes = int(nbytes)
         self.buf = torch.empty(self.nbytes, dtype=torch.uint8, device=device)
 

@@ -684,11 +684,17 @@ int syevd(long n, long b, long nb, const double* A, long lda, double* w, double*
 }
 
 // Mixed form: workspace = the plain solve's (any order) + the integer part.
-size_t syevd_mixed_ws_bytes(long n, long b, long nb, int nmod, int refine_iters) {
+// The full workspace (with the split buffer and the own integer workspaces
+// up to kMixedDcOwnMax) and the minimum one (one stage-2 chain, the D&C after
+// the Q1 formation), for callers short of device memory.
+size_t syevd_mixed_ws_min_bytes(long n, long b, long nb, int nmod, int refine_iters) {
   const size_t plain = (syevd_any_ws_bytes(n, b, nb) + 255) / 256 * 256;
   const long np = padded_order(n, nb);
-  return plain + (size_t)mixed_oz_bytes(np, nb, nmod, refine_iters) + 256 +
-         (size_t)mixed_extra(np, nb, nmod).total;
+  return plain + (size_t)mixed_oz_bytes(np, nb, nmod, refine_iters) + 256;
+}
+size_t syevd_mixed_ws_bytes(long n, long b, long nb, int nmod, int refine_iters) {
+  return syevd_mixed_ws_min_bytes(n, b, nb, nmod, refine_iters) +
+         (size_t)mixed_extra(padded_order(n, nb), nb, nmod).total;
 }
 
 int syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, double* X,
@@ -701,8 +707,9 @@ int syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, d
   const long np = padded_order(n, nb);
   if (refine_iters > 0 && np > 65535) return EVD_ERR_INVALID_ARG;
   if (lda < n || ldX < n || !A || !w || !X || !work) return EVD_ERR_INVALID_ARG;
-  if ((size_t)lwork_bytes < syevd_mixed_ws_bytes(n, b, nb, nmod, refine_iters))
+  if ((size_t)lwork_bytes < syevd_mixed_ws_min_bytes(n, b, nb, nmod, refine_iters))
     return EVD_ERR_WORKSPACE;
+  const bool full = (size_t)lwork_bytes >= syevd_mixed_ws_bytes(n, b, nb, nmod, refine_iters);
   const size_t plain = (syevd_any_ws_bytes(n, b, nb) + 255) / 256 * 256;
   uint8_t* wb = reinterpret_cast<uint8_t*>(work);
   uint8_t* ozb = reinterpret_cast<uint8_t*>(((uintptr_t)(wb + plain) + 255) & ~(uintptr_t)255);
@@ -710,7 +717,7 @@ int syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, d
   const MixedExtra xt = mixed_extra(np, nb, nmod);
   uint8_t* xb = reinterpret_cast<uint8_t*>(((uintptr_t)(ozb + ozn) + 255) & ~(uintptr_t)255);
   MixedOpts mx{nmod, refine_iters, moduli_update, ozb, ozn, nullptr, 0, nullptr, 0, nullptr};
-  if (xt.total > 0) {
+  if (full && xt.total > 0) {
     mx.oz_dc = xb;
     mx.oz_dc_bytes = xt.dc;
     mx.oz_q1 = xb + xt.dc;
@@ -776,6 +783,14 @@ extern "C" long evd_syevd_mixed_work_size(long n, long b, long nb, int moduli, i
       refine_iters < 0)
     return 0;
   return (long)evd::syevd_mixed_ws_bytes(n, b, nb, moduli, refine_iters);
+}
+
+extern "C" long evd_syevd_mixed_work_size_min(long n, long b, long nb, int moduli,
+                                              int refine_iters) {
+  if (!evd::shape_ok(n, b, nb) || moduli < evd::kOzMinMod || moduli > evd::kOzMaxMod ||
+      refine_iters < 0)
+    return 0;
+  return (long)evd::syevd_mixed_ws_min_bytes(n, b, nb, moduli, refine_iters);
 }
 
 extern "C" int evd_syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w,

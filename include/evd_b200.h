@@ -315,6 +315,11 @@ int evd_syevd_batched(long count, const long* n, const double* const* A, const l
  * refine_iters > 0 needs n <= 65535 (padded order).  work:
  * evd_syevd_mixed_work_size bytes.  Synchronises `stream`. */
 long evd_syevd_mixed_work_size(long n, long b, long nb, int moduli, int refine_iters);
+/* The smallest workspace evd_syevd_mixed accepts (no counterpart in the
+ * reference): with less than evd_syevd_mixed_work_size bytes it runs one
+ * stage-2 chain and the divide and conquer after the Q1 formation, the
+ * schedule of orders above 24576 (slower, about 2.4 n^2 + n^2 doubles less). */
+long evd_syevd_mixed_work_size_min(long n, long b, long nb, int moduli, int refine_iters);
 int evd_syevd_mixed(long n, long b, long nb, const double* A, long lda, double* w, double* X,
                     long ldX, int moduli, int refine_iters, int moduli_update, void* work,
                     long lwork_bytes, int timed, cudaStream_t stream);

@@ -87,3 +87,37 @@ def test_mixed_matches_reference_build(cuda, evdlib):
     X8 = X[:, :8].cpu().numpy()
     s = np.sign(np.sum(X8 * f["X8"], axis=0))
     assert np.abs(X8 - f["X8"] * s).max() <= 1e-9
+
+
+@pytest.mark.parametrize("n,nb,moduli,iters", [(1024, 256, 14, 0), (1500, 256, 14, 0),
+                                               (2048, 512, 8, 2)])
+def test_mixed_minimal_workspace_one_chain(cuda, evdlib, n, nb, moduli, iters):
+    """With the smallest workspace the solve runs one stage-2 chain and the
+    divide and conquer after the Q1 formation (the schedule of orders above
+    24576): same bars, same eigenvalues as the full-workspace schedule."""
+    A = O.sym_gaussian(n, seed=n + 17)
+    nA = np.linalg.norm(A, 2)
+    Ad = evdlib.to_cm(torch.from_numpy(A), device=cuda)
+    lmin = evdlib.lib().evd_syevd_mixed_work_size_min(n, 32, nb, moduli, iters)
+    lfull = evdlib.lib().evd_syevd_mixed_work_size(n, 32, nb, moduli, iters)
+    assert 0 < lmin < lfull
+    wsm = evdlib.MixedWorkspace(n, 32, nb, moduli, iters, device=cuda, minimal=True)
+    assert wsm.nbytes == lmin
+    w1, X1 = evdlib.syevd_mixed(Ad, 32, nb, moduli, iters, ws=wsm)
+    w2, X2 = evdlib.syevd_mixed(Ad, 32, nb, moduli, iters)
+    r1, o1 = evdlib.check_eig(Ad, w1, X1)
+    r2, o2 = evdlib.check_eig(Ad, w2, X2)
+    torch.cuda.synchronize()
+    assert r1 <= 1e-13 and o1 <= 1e-13, (r1, o1)
+    assert r2 <= 1e-13 and o2 <= 1e-13, (r2, o2)
+    w1, w2 = w1.cpu().numpy(), w2.cpu().numpy()
+    assert np.abs(w1 - np.linalg.eigvalsh(A)).max() <= 1e-12 * nA
+    assert np.abs(w1 - w2).max() <= 1e-13 * nA
+    # one byte short of the minimum is rejected before any device work
+    short = torch.empty(lmin - 1, dtype=torch.uint8, device=cuda)
+    wd = torch.empty(n, dtype=torch.float64, device=cuda)
+    Xd = evdlib.empty_cm(n, n, device=cuda)
+    rc = evdlib.lib().evd_syevd_mixed(n, 32, nb, Ad.data_ptr(), n, wd.data_ptr(),
+                                      Xd.data_ptr(), n, moduli, iters, 14, short.data_ptr(),
+                                      lmin - 1, 0, None)
+    assert rc == -5  # EVD_ERR_WORKSPACE
