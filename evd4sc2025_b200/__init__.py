@@ -43,7 +43,7 @@ __all__ = [
     "q_from_wy", "sbr_back", "check_orthogonality", "check_eig", "syevd", "last_timings",
     "syevd_values", "eigvalsh", "stebz", "refine_syev", "refine_work", "dgemm_ozaki",
     "dgemm_ozaki_work_size", "ozaki_bits", "refine_syev_ozaki", "refine_ozaki_work",
-    "syevd_mixed", "MixedWorkspace", "last_refine_ms", "mixed_last_timings",
+    "syevd_mixed", "syevd_s", "MixedWorkspace", "last_refine_ms", "mixed_last_timings",
     # reference-named aliases
     "my_ZY_ZY_SBR_Vector", "panelQR", "hou_tsqr_panel", "tc_ozimmu_syr2k",
     "my_BC_back_trans_v8_10_noBandU", "computerWYFromSlide", "computerQFromWY",
@@ -80,10 +80,10 @@ def to_cm(t: torch.Tensor, device="cuda", ld: int | None = None) -> torch.Tensor
     return out
 
 
-def _cm(t: torch.Tensor, name: str):
-    """(pointer, leading dimension) of a column-major FP64 CUDA matrix."""
-    if t.dtype != F64:
-        raise TypeError(f"{name} must be float64")
+def _cm(t: torch.Tensor, name: str, dtype=F64):
+    """(pointer, leading dimension) of a column-major CUDA matrix of `dtype`."""
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {str(dtype).replace('torch.', '')}")
     if not t.is_cuda:
         raise ValueError(f"{name} must be a CUDA tensor")
     if t.dim() == 1:
@@ -456,6 +456,30 @@ def syevd_mixed(A: torch.Tensor, b: int = 32, nb: int = 1024, moduli: int = 14,
     px, ldx = _cm(X, "X")
     call("evd_syevd_mixed", n, b, nb, pa, lda, _ptr(w), px, ldx, moduli, refine_iters,
          moduli_update, _ptr(ws.buf), ws.nbytes, 1 if timed else 0, _stream(stream))
+    return w, X
+
+
+def syevd_s(A: torch.Tensor, b: int = 32, nb: int = 1024, work: torch.Tensor | None = None,
+            stream=None, w: torch.Tensor | None = None, X: torch.Tensor | None = None):
+    """All eigenpairs of the symmetric FP32 matrix A (column-major), in FP32:
+    the mixed form of the solve with 8 moduli and no refinement (the
+    contractions on the integer tensor cores at FP32 accuracy; panels, chase
+    and divide and conquer in FP64).  A is not modified."""
+    n = A.shape[0]
+    dev = A.device
+    nbytes = int(lib().evd_syevd_s_work_size(n, b, nb))
+    if nbytes <= 0:
+        raise ValueError("unsupported shape")
+    if work is None or work.numel() < nbytes:
+        work = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    if w is None:
+        w = torch.empty(n, dtype=torch.float32, device=dev)
+    if X is None:
+        X = empty_cm(n, n, device=dev, dtype=torch.float32)
+    pa, lda = _cm(A, "A", torch.float32)
+    px, ldx = _cm(X, "X", torch.float32)
+    call("evd_syevd_s", n, b, nb, pa, lda, _ptr(w), px, ldx, _ptr(work), work.numel(),
+         _stream(stream))
     return w, X
 
 

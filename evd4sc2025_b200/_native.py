@@ -56,6 +56,8 @@ SIGNATURES = {
     "evd_syevd_values": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _p]),
     "evd_syevd": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _i, _p]),
     "evd_syevd_mixed_work_size": (_l, [_l, _l, _l, _i, _i]),
+    "evd_syevd_s_work_size": (_l, [_l, _l, _l]),
+    "evd_syevd_s": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _p, _l, _p]),
     "evd_syevd_mixed_work_size_min": (_l, [_l, _l, _l, _i, _i]),
     "evd_syevd_mixed": (_i, [_l, _l, _l, _p, _l, _p, _p, _l, _i, _i, _i, _p, _l, _i, _p]),
     "evd_syevd_last_refine_ms": (_d, []),

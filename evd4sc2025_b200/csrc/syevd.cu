@@ -350,7 +350,9 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
   const OzWork ozdc{mx->nmod, mx->oz_dc, mx->oz_dc_bytes};
   const OzWork ozq1{mx->nmod, mx->oz_q1, mx->oz_q1_bytes};
   const bool dc_own = mx->oz_dc != nullptr;
-  if ((size_t)q2_tbuf_doubles(n) > (size_t)n * n) return EVD_ERR_WORKSPACE;
+  // the chains' T factors go into OA (free after stage 1); for very small n
+  // they do not fit and the stage-2 kernel rebuilds them itself
+  double* tbuf = ((size_t)q2_tbuf_doubles(n) <= (size_t)n * n) ? OA : nullptr;
   double* XA = mx->split_buf;  // chain A, then Q^T
   const bool split = XA != nullptr && n > 64;
   const long k = split ? std::max(8L, (long)(0.39 * (double)n) / 8 * 8) : 0;
@@ -421,8 +423,8 @@ static int syevd_mixed_core(long n, long b, long nb, const double* A, long lda, 
       const bool in_b = split && bounds[i] >= k;
       cudaStream_t s2 = in_b ? sc : sa;
       EVD_CUDA_TRY(cudaStreamWaitEvent(s2, evr[i], 0));
-      EVD_TRY(q2_apply_range(true, n, n, U, n, in_b ? X : PA, in_b ? ldX : ldPA, OA, bounds[i],
-                             bounds[i + 1], in_b ? k : 0, s2));
+      EVD_TRY(q2_apply_range(true, n, n, U, n, in_b ? X : PA, in_b ? ldX : ldPA, tbuf,
+                             bounds[i], bounds[i + 1], in_b ? k : 0, s2));
     }
   }
   EVD_CUDA_TRY(cudaEventRecord(ev[5], sa));
@@ -800,6 +802,84 @@ extern "C" int evd_syevd_mixed(long n, long b, long nb, const double* A, long ld
   try {
     return evd::syevd_mixed(n, b, nb, A, lda, w, X, ldX, moduli, refine_iters, moduli_update,
                             work, lwork_bytes, timed, stream);
+  } catch (...) {
+    return EVD_ERR_HOST;
+  }
+}
+
+// ---- FP32 solve ----
+// FP32 matrices in and out.  The contractions that dominate the work (the
+// stage-1 trailing SYR2K, the Q1 formation, the large merges and the products
+// that form X) run as emulated products with kFp32Moduli moduli (30-bit
+// operands, no refinement), i.e. the mixed form at the accuracy FP32 needs;
+// the panels, the chase and the divide and conquer stay FP64: they are
+// latency-bound, so narrower arithmetic would not make them faster.  The
+// workspace holds FP64 copies of A, w and X before the mixed form's own.
+namespace evd {
+namespace {
+
+constexpr int kFp32Moduli = 8;
+
+template <typename S, typename D>
+__global__ void convert_kernel(long m, long n, const S* __restrict__ src, long lds,
+                               D* __restrict__ dst, long ldd) {
+  for (long j = blockIdx.y; j < n; j += gridDim.y)
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < m;
+         i += (long)gridDim.x * blockDim.x)
+      dst[i + j * ldd] = (D)src[i + j * lds];
+}
+
+template <typename S, typename D>
+int convert(long m, long n, const S* src, long lds, D* dst, long ldd, cudaStream_t st) {
+  if (m <= 0 || n <= 0) return EVD_SUCCESS;
+  dim3 grid(ceil_div_i(m, 256), (unsigned)std::min<long>(n, 65535));
+  convert_kernel<S, D><<<grid, 256, 0, st>>>(m, n, src, lds, dst, ldd);
+  EVD_LAUNCHED();
+  return EVD_SUCCESS;
+}
+
+size_t al256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+size_t syevd_s_ws_bytes(long n, long b, long nb) {
+  const size_t sq = al256(sizeof(double) * (size_t)n * n);
+  return 2 * sq + al256(sizeof(double) * (size_t)n) +
+         syevd_mixed_ws_bytes(n, b, nb, kFp32Moduli, 0) + 256;
+}
+
+int syevd_s(long n, long b, long nb, const float* A, long lda, float* w, float* X, long ldX,
+            void* work, long lwork_bytes, cudaStream_t st) {
+  if (!shape_ok(n, b, nb)) return EVD_ERR_INVALID_ARG;
+  if (lda < n || ldX < n || !A || !w || !X || !work) return EVD_ERR_INVALID_ARG;
+  if ((size_t)lwork_bytes < syevd_s_ws_bytes(n, b, nb)) return EVD_ERR_WORKSPACE;
+  uint8_t* p = reinterpret_cast<uint8_t*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  const size_t sq = al256(sizeof(double) * (size_t)n * n);
+  double* Ad = reinterpret_cast<double*>(p);
+  double* Xd = reinterpret_cast<double*>(p + sq);
+  double* wd = reinterpret_cast<double*>(p + 2 * sq);
+  uint8_t* mw = p + 2 * sq + al256(sizeof(double) * (size_t)n);
+  const size_t mbytes = syevd_mixed_ws_bytes(n, b, nb, kFp32Moduli, 0);
+  EVD_TRY(convert(n, n, A, lda, Ad, n, st));
+  EVD_TRY(syevd_mixed(n, b, nb, Ad, n, wd, Xd, n, kFp32Moduli, 0, kFp32Moduli, mw, (long)mbytes,
+                      0, st));
+  EVD_TRY(convert(n, 1, wd, n, w, n, st));
+  EVD_TRY(convert(n, n, Xd, n, X, ldX, st));
+  EVD_CUDA_TRY(cudaStreamSynchronize(st));
+  return EVD_SUCCESS;
+}
+
+}  // namespace evd
+
+extern "C" long evd_syevd_s_work_size(long n, long b, long nb) {
+  if (!evd::shape_ok(n, b, nb)) return 0;
+  return (long)evd::syevd_s_ws_bytes(n, b, nb);
+}
+
+extern "C" int evd_syevd_s(long n, long b, long nb, const float* A, long lda, float* w, float* X,
+                           long ldX, void* work, long lwork_bytes, cudaStream_t stream) {
+  try {
+    return evd::syevd_s(n, b, nb, A, lda, w, X, ldX, work, lwork_bytes, stream);
   } catch (...) {
     return EVD_ERR_HOST;
   }

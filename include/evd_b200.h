@@ -334,6 +334,23 @@ double evd_syevd_last_refine_ms(void);
  * chase and the divide and conquer. */
 void evd_syevd_mixed_last_timings(double out_ms[8]);
 
+/* ---- FP32 solve ---------------------------------------------------------- */
+
+/* The reference's driver is FP64 only (myEVD.cu:251-706); its FP32 pieces are
+ * panelQR<float> (api/panelQR.cu:262-464) and tc_ozimmu_syr2k<float>
+ * (api/TCblas/tc_ozimmu_syr2k.cu:343-629).  All eigenpairs of the symmetric
+ * FP32 matrix A (n x n, lda; any n >= 1): w (n, ascending) and X (n x n, ldX),
+ * FP32, device pointers.  The solve is evd_syevd_mixed with 8 moduli (30-bit
+ * operands) and no refinement: the dominant contractions run on the integer
+ * tensor cores at the accuracy FP32 needs, while the latency-bound stages
+ * (panels, chase, divide and conquer) stay FP64.  Residual and orthogonality
+ * (1/n normalised) are FP32-level or better.  work: evd_syevd_s_work_size
+ * bytes (FP64 copies of A, w and X plus the mixed form's workspace).
+ * Synchronises `stream`. */
+long evd_syevd_s_work_size(long n, long b, long nb);
+int evd_syevd_s(long n, long b, long nb, const float* A, long lda, float* w, float* X, long ldX,
+                void* work, long lwork_bytes, cudaStream_t stream);
+
 /* ---- Iterative refinement of eigenpairs -------------------------------- */
 
 /* No counterpart in the reference.  Ogita-Aishima refinement (RefSyEv,

@@ -77,6 +77,17 @@ def test_mixed_any_order(cuda, evdlib):
     assert np.abs(np.sort(w) - np.linalg.eigvalsh(A)).max() <= 1e-12 * np.linalg.norm(A, 2)
 
 
+@pytest.mark.parametrize("n,nb,moduli,iters", [(1, 64, 14, 0), (5, 64, 14, 0), (64, 64, 14, 0),
+                                               (100, 64, 8, 2), (300, 128, 14, 1)])
+def test_mixed_small_orders(cuda, evdlib, n, nb, moduli, iters):
+    """Orders whose stage-2 T factors do not fit in the borrowed n x n buffer
+    (the kernel then rebuilds them) and orders padded to 64."""
+    A = O.sym_gaussian(n, seed=n + 3)
+    w, X, res, orth = _solve(evdlib, cuda, A, nb, moduli=moduli, refine_iters=iters)
+    assert res <= 1e-13 and orth <= 1e-13, (res, orth)
+    assert np.abs(w - np.linalg.eigvalsh(A)).max() <= 1e-12 * max(np.linalg.norm(A, 2), 1.0)
+
+
 def test_mixed_matches_reference_build(cuda, evdlib):
     f = np.load(GOLD / "ref_n4096_s13.npz")
     n, seed = int(f["n"]), int(f["seed"])
