@@ -97,6 +97,20 @@ def test_workspace_too_small_reported_without_gpu(evdlib):
     assert lib.evd_panel_qr_s(128, 32, 256, 128, 256, 128, 256, 32, 256, 10, None) == -5
 
 
+def test_fp32_solve_queries_without_gpu(evdlib):
+    lib = evdlib.lib()
+    for n, nb in ((1, 64), (100, 64), (4096, 1024)):
+        need = lib.evd_syevd_s_work_size(n, 32, nb)
+        # FP64 copies of A, X and w on top of the 8-moduli mixed workspace
+        assert need >= lib.evd_syevd_mixed_work_size(n, 32, nb, 8, 0) + 16 * n * n + 8 * n
+    assert lib.evd_syevd_s_work_size(100, 16, 64) == 0           # b = 32 only
+    assert lib.evd_syevd_s_work_size(0, 32, 64) == 0
+    assert lib.evd_syevd_s_work_size(100, 32, 96) == 0           # nb = 32 * 2^k
+    # argument errors are reported before any device work
+    assert lib.evd_syevd_s(100, 32, 64, None, 100, None, None, 100, None, 0, None) == -1
+    assert lib.evd_syevd_s(100, 32, 64, 8, 99, 8, 8, 100, 8, 1 << 30, None) == -1
+
+
 def test_batched_queries_without_gpu(evdlib):
     lib = evdlib.lib()
     n = (C.c_long * 3)(100, 1000, 64)
