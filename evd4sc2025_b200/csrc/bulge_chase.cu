@@ -56,37 +56,6 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Thread 0 waits until *flag >= target (or an error is raised elsewhere); the
-// result is broadcast through shared memory.  false = abandon the sweep.
-__device__ bool cta_wait_geq(const int* flag, int target, int* err, volatile int* s_ok) {
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    if (ld_acquire(flag) < target) {
-      unsigned long long t0 = globaltimer_ns();
-      unsigned spins = 0;
-      while (ld_acquire(flag) < target) {
-        __nanosleep(32);
-        if ((++spins & 31u) == 0) {
-          if (*(volatile int*)err != 0) {
-            ok = 0;
-            break;
-          }
-          if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
-            atomicCAS(err, 0, kDevTimeoutChase);
-            ok = 0;
-            break;
-          }
-        }
-      }
-    }
-    *s_ok = ok;
-  }
-  __syncthreads();
-  const bool ok = *s_ok != 0;
-  __syncthreads();  // nobody rewrites s_ok before everyone has read it
-  return ok;
-}
-
 // All threads' prior writes -> visible at gpu scope, then thread 0 publishes.
 __device__ __forceinline__ void cta_publish(int* flag, int value) {
   __syncthreads();
@@ -152,9 +121,34 @@ struct ChaseSmem {
   double u[kBW];
   double v[kBW];
   double red[4];
-  int ok;
   int ticket;
 };
+
+// Thread 0 waits until *flag >= target (or an error is raised elsewhere); the
+// barrier itself (__syncthreads_and) gives every thread the verdict.
+// false = abandon the sweep.
+__device__ bool cta_wait_and(const int* flag, int target, int* err) {
+  int ok = 1;
+  if (threadIdx.x == 0 && ld_acquire(flag) < target) {
+    unsigned long long t0 = globaltimer_ns();
+    unsigned spins = 0;
+    while (ld_acquire(flag) < target) {
+      __nanosleep(32);
+      if ((++spins & 31u) == 0) {
+        if (*(volatile int*)err != 0) {
+          ok = 0;
+          break;
+        }
+        if (globaltimer_ns() - t0 > kWaitTimeoutNs) {
+          atomicCAS(err, 0, kDevTimeoutChase);
+          ok = 0;
+          break;
+        }
+      }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
+}
 
 __global__ void __launch_bounds__(kChaseThreads)
     chase_kernel(int n, double* __restrict__ sub, double* __restrict__ U, long ldU, int* prog,
@@ -180,7 +174,7 @@ __global__ void __launch_bounds__(kChaseThreads)
     int rb = min(kBW, (int)(n - r));
     int cb = 1;  // columns of the previous tile (B1): 1 at the first step
     int cur = 0;
-    if (s > 0 && !cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) break;
+    if (s > 0 && !cta_wait_and(prog + s - 1, (int)(r + 2 * kBW), err)) break;
     // previous tile = column s (its offsets 1..rb hold B1 = A(r:r+rb, s))
     tile_load_async(sm.tile[1 - cur], sub, s, 1);
     cp_async_commit_wait_all();
@@ -262,16 +256,16 @@ __global__ void __launch_bounds__(kChaseThreads)
         double uy = (p == 0) ? sm.u[i] * y : 0.0;
         uy = warp_sum_tc(uy);
         if (lane == 0) sm.red[warp] = uy;
+        if (p == 0) sm.v[i] = y;  // y here; v_j = y_j - t u_j / 2 is formed below
         __syncthreads();
         const double t = (sm.red[0] + sm.red[1]) + (sm.red[2] + sm.red[3]);
         const double vi = y - 0.5 * t * sm.u[i];
-        if (p == 0) sm.v[i] = vi;
-        __syncthreads();
         const double ui = sm.u[i];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int j = 8 * p + k;
-          if (j <= i && i < rb) T[j * kOff + (i - j)] -= ui * sm.v[j] + vi * sm.u[j];
+          const double vj = sm.v[j] - 0.5 * t * sm.u[j];
+          if (j <= i && i < rb) T[j * kOff + (i - j)] -= ui * vj + vi * sm.u[j];
         }
       }
       // (6) B1' <- B1' H : row i = q (rows r+rb+i), N(i, j) = T[j][rb + i - j].
@@ -307,7 +301,7 @@ __global__ void __launch_bounds__(kChaseThreads)
       // by all four warps in (6): the wait below ends with a CTA barrier; sweep
       // 0 waits on nobody and takes the barrier alone
       if (s > 0) {
-        if (!cta_wait_geq(prog + s - 1, (int)(r + 2 * kBW), err, &sm.ok)) {
+        if (!cta_wait_and(prog + s - 1, (int)(r + 2 * kBW), err)) {
           alive = false;
           break;
         }
